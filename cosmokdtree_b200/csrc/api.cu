@@ -1,0 +1,320 @@
+// api.cu -- the extern "C" boundary of libckd (declared in include/ckd.h).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ckd_common.cuh"
+
+namespace ckd {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+ckd_status fail(ckd_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+ckd_status cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky-free error so later calls can proceed
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return CKD_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ||
+      e == cudaErrorNoKernelImageForDevice)
+    return CKD_ERR_NO_DEVICE;
+  return CKD_ERR_CUDA;
+}
+
+// ---------------------------------------------------------- scratch memory
+// One stream-ordered pool per device, keeping freed blocks cached.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64];
+static bool g_pool_ok[64];
+
+static cudaError_t pool_for_current(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool_ok[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    e = cudaMemPoolCreate(&g_pool[dev], &props);
+    if (e != cudaSuccess) return e;
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &thr);
+    g_pool_ok[dev] = true;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool;
+  cudaError_t e = pool_for_current(&pool);
+  if (e != cudaSuccess) return e;
+  if (bytes == 0) bytes = 16;
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+cudaError_t dev_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
+
+ckd_status build_dispatch(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t s);
+ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
+                   int64_t* idx, cudaStream_t s);
+ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
+                    int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
+                    cudaStream_t s);
+ckd_status box_run(const ckd_tree* t, const double* boxes, int64_t nb, bool fill, int64_t* counts,
+                   const int64_t* offsets, int64_t* idx, cudaStream_t s);
+
+static ckd_status check_device(int* dev_out) {
+  int dev = 0;
+  CKD_CUDA(cudaGetDevice(&dev));
+  int major = 0;
+  CKD_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major != 10) return fail(CKD_ERR_NO_DEVICE, "libckd is built for sm_100a (B200) devices only");
+  if (dev_out) *dev_out = dev;
+  return CKD_OK;
+}
+
+static ckd_status check_tree(const ckd_tree* t) {
+  if (!t) return fail(CKD_ERR_BAD_ARG, "null tree handle");
+  int dev = 0;
+  CKD_CUDA(cudaGetDevice(&dev));
+  if (dev != t->device) return fail(CKD_ERR_BAD_ARG, "the current device is not the tree's device");
+  return CKD_OK;
+}
+
+static void release_tree(ckd_tree* t) {
+  if (!t) return;
+  cudaFree(t->meta);
+  cudaFree(t->box);
+  cudaFree(t->cell);
+  cudaFree(t->pts);
+  cudaFree(t->ids);
+  delete t;
+}
+
+}  // namespace ckd
+
+using namespace ckd;
+
+extern "C" {
+
+int ckd_version(void) { return 100; }
+
+const char* ckd_last_error(void) { return g_err.c_str(); }
+
+ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf, const double* boxsize,
+                     int pts_on_device, void* stream, ckd_tree** out) {
+  if (!out) return fail(CKD_ERR_BAD_ARG, "null output handle pointer");
+  *out = nullptr;
+  if (!pts) return fail(CKD_ERR_BAD_ARG, "null points pointer");
+  if (n < 1) return fail(CKD_ERR_BAD_ARG, "at least one point is required");
+  if (n >= 0x7fffffffll) return fail(CKD_ERR_BAD_ARG, "more than 2^31-2 points are not supported");
+  if (d < 1 || d > CKD_MAX_D) return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+  if (leaf < 1) return fail(CKD_ERR_BAD_ARG, "Leaf size must be a positive integer");
+  if (dtype != CKD_F64 && dtype != CKD_F32) return fail(CKD_ERR_BAD_ARG, "dtype must be F64 or F32");
+  int dev = 0;
+  CKD_TRY(check_device(&dev));
+  cudaStream_t s = (cudaStream_t)stream;
+  ckd_tree* t = new ckd_tree();
+  t->device = dev;
+  t->n = n;
+  t->d = d;
+  t->leaf = leaf;
+  t->input_dtype = dtype;
+  if (boxsize) {
+    t->periodic = 1;
+    for (int j = 0; j < d; ++j) {
+      if (!(boxsize[j] > 0) || !std::isfinite(boxsize[j])) {
+        delete t;
+        return fail(CKD_ERR_BAD_ARG, "boxsize entries must be positive and finite");
+      }
+      t->L[j] = boxsize[j];
+    }
+  }
+  const void* src = pts;
+  void* staging = nullptr;
+  size_t esz = dtype == CKD_F32 ? 4 : 8;
+  ckd_status st = CKD_OK;
+  if (!pts_on_device) {
+    cudaError_t e = dev_alloc(&staging, esz * n * d, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(staging, pts, esz * n * d, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = cuda_fail(e, "copying points to the device");
+    src = staging;
+  }
+  if (st == CKD_OK) st = build_dispatch(t, src, dtype, s);
+  if (staging) dev_free(staging, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (st == CKD_OK && e != cudaSuccess) st = cuda_fail(e, "build");
+  if (st != CKD_OK) {
+    release_tree(t);
+    return st;
+  }
+  *out = t;
+  return CKD_OK;
+}
+
+ckd_status ckd_free(ckd_tree* tree) {
+  if (!tree) return CKD_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(tree->device);
+  release_tree(tree);
+  cudaSetDevice(cur);
+  return CKD_OK;
+}
+
+ckd_status ckd_tree_info(const ckd_tree* t, int64_t* n, int* d, int* leaf, int* periodic,
+                         int32_t* n_nodes, int32_t* n_leaves, int32_t* depth, int* device) {
+  if (!t) return fail(CKD_ERR_BAD_ARG, "null tree handle");
+  if (n) *n = t->n;
+  if (d) *d = t->d;
+  if (leaf) *leaf = t->leaf;
+  if (periodic) *periodic = t->periodic;
+  if (n_nodes) *n_nodes = t->n_nodes;
+  if (n_leaves) *n_leaves = t->n_leaves;
+  if (depth) *depth = t->depth;
+  if (device) *device = t->device;
+  return CKD_OK;
+}
+
+ckd_status ckd_tree_export(const ckd_tree* t, int32_t* axis, double* split, int64_t* start,
+                           int64_t* count, int64_t* left, int64_t* right, double* cell, double* box,
+                           int64_t* ids) {
+  CKD_TRY(check_tree(t));
+  const int m = t->n_nodes, d2 = 2 * t->d;
+  std::vector<NodeMeta> meta(m);
+  std::vector<double> hc((size_t)m * d2), hb((size_t)m * d2);
+  CKD_CUDA(cudaMemcpy(meta.data(), t->meta, sizeof(NodeMeta) * m, cudaMemcpyDeviceToHost));
+  if (cell) CKD_CUDA(cudaMemcpy(hc.data(), t->cell, sizeof(double) * m * d2, cudaMemcpyDeviceToHost));
+  if (box) CKD_CUDA(cudaMemcpy(hb.data(), t->box, sizeof(double) * m * d2, cudaMemcpyDeviceToHost));
+  if (ids) {
+    std::vector<int32_t> hi(t->n);
+    CKD_CUDA(cudaMemcpy(hi.data(), t->ids, sizeof(int32_t) * t->n, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < t->n; ++i) ids[i] = hi[i];
+  }
+  // preorder, left subtree first
+  std::vector<int32_t> pre(m, -1);
+  std::vector<int32_t> order;
+  order.reserve(m);
+  std::vector<int32_t> st{0};
+  while (!st.empty()) {
+    int32_t a = st.back();
+    st.pop_back();
+    pre[a] = (int32_t)order.size();
+    order.push_back(a);
+    if (meta[a].left >= 0) {
+      st.push_back(meta[a].left + 1);
+      st.push_back(meta[a].left);
+    }
+  }
+  if ((int)order.size() != m) return fail(CKD_ERR_CUDA, "internal error: tree is not connected");
+  for (int i = 0; i < m; ++i) {
+    const NodeMeta& x = meta[order[i]];
+    bool lf = x.left < 0;
+    if (axis) axis[i] = lf ? -1 : x.axis;
+    if (split) split[i] = lf ? 0.0 : x.split;
+    if (start) start[i] = x.start;
+    if (count) count[i] = x.count;
+    if (left) left[i] = lf ? -1 : pre[x.left];
+    if (right) right[i] = lf ? -1 : pre[x.left + 1];
+    if (cell) std::memcpy(cell + (size_t)i * d2, &hc[(size_t)order[i] * d2], sizeof(double) * d2);
+    if (box) std::memcpy(box + (size_t)i * d2, &hb[(size_t)order[i] * d2], sizeof(double) * d2);
+  }
+  return CKD_OK;
+}
+
+ckd_status ckd_knn(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
+                   int64_t* idx, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  return knn_run(t, q, nq, k, sorted, dist, idx, (cudaStream_t)stream);
+}
+
+ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                        double* dist, int64_t* idx, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  double *dq = nullptr, *dd = nullptr;
+  int64_t* di = nullptr;
+  CKD_CUDA(dev_alloc((void**)&dq, sizeof(double) * nq * t->d, s));
+  CKD_CUDA(dev_alloc((void**)&dd, sizeof(double) * nq * k, s));
+  CKD_CUDA(dev_alloc((void**)&di, sizeof(int64_t) * nq * k, s));
+  CKD_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * nq * t->d, cudaMemcpyHostToDevice, s));
+  ckd_status st = knn_run(t, dq, nq, k, sorted, dd, di, s);
+  if (st == CKD_OK) {
+    CKD_CUDA(cudaMemcpyAsync(dist, dd, sizeof(double) * nq * k, cudaMemcpyDeviceToHost, s));
+    CKD_CUDA(cudaMemcpyAsync(idx, di, sizeof(int64_t) * nq * k, cudaMemcpyDeviceToHost, s));
+  }
+  dev_free(dq, s);
+  dev_free(dd, s);
+  dev_free(di, s);
+  CKD_CUDA(cudaStreamSynchronize(s));
+  return st;
+}
+
+ckd_status ckd_ball_count(const ckd_tree* t, const double* q, int64_t nq, double radius,
+                          int64_t* counts, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (!(radius > 0) || !std::isfinite(radius))
+    return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !counts) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  return ball_run(t, q, nq, radius, false, 0, counts, nullptr, nullptr, nullptr,
+                  (cudaStream_t)stream);
+}
+
+ckd_status ckd_ball_fill(const ckd_tree* t, const double* q, int64_t nq, double radius, int sorted,
+                         const int64_t* offsets, int64_t* idx, double* dist, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (!(radius > 0) || !std::isfinite(radius))
+    return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !offsets || !idx || !dist) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  return ball_run(t, q, nq, radius, true, sorted, nullptr, offsets, idx, dist,
+                  (cudaStream_t)stream);
+}
+
+ckd_status ckd_box_count(const ckd_tree* t, const double* boxes, int64_t nb, int64_t* counts,
+                         void* stream) {
+  CKD_TRY(check_tree(t));
+  if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
+  if (nb == 0) return CKD_OK;
+  if (!boxes || !counts) return fail(CKD_ERR_BAD_ARG, "null box or output pointer");
+  return box_run(t, boxes, nb, false, counts, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+ckd_status ckd_box_fill(const ckd_tree* t, const double* boxes, int64_t nb, const int64_t* offsets,
+                        int64_t* idx, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
+  if (nb == 0) return CKD_OK;
+  if (!boxes || !offsets || !idx) return fail(CKD_ERR_BAD_ARG, "null box or output pointer");
+  return box_run(t, boxes, nb, true, nullptr, offsets, idx, (cudaStream_t)stream);
+}
+
+ckd_status ckd_exclusive_scan(const int64_t* in, int64_t* out, int64_t n, void* stream) {
+  if (n < 0 || !out || (n > 0 && !in)) return fail(CKD_ERR_BAD_ARG, "bad scan arguments");
+  return scan_i64(in, out, n, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,335 @@
+// ball_box.cu -- ball (radius) and axis-aligned box searches, two-phase CSR.
+//
+// Ball (cosmokdtree.f90:1015-1212): a point is a result iff its FP64 squared
+// distance (reference arithmetic) is <= radius^2 (inclusive, :1126, :1175).  The
+// reference's "fully inside" shortcut (:1116-1118, :1332-1366) selects exactly
+// the same points, because a node's max-distance bound is never below the
+// computed distance of a point inside it; the count pass uses it (with the
+// tight box) to skip distance work.  Traversal is left child first, so the
+// unsorted order of a row is the reference's non-periodic order (left-first DFS,
+// leaf order).  sorted=1 orders each row by (d2, id).
+//
+// Box (cosmokdtree.f90:1220-1328): descend left iff box_lo[axis] < split, right
+// iff box_hi[axis] > split (strict), leaf test lo <= x <= hi on every axis
+// (inclusive), no periodic wrap.  Each lane carries one box; the warp walks the
+// union of the lanes' paths with a per-entry lane mask, left first, so every
+// row comes out in the reference's order.
+#include <algorithm>
+
+#include "ckd_common.cuh"
+#include "ckd_traverse.cuh"
+
+namespace ckd {
+
+namespace {
+
+constexpr int kStack = 96;
+
+template <int D, bool PER, bool FILL>
+__global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restrict__ Q,
+                                              const int32_t* __restrict__ order, int64_t nq,
+                                              double r2, int32_t* __restrict__ gstack,
+                                              int stack_len, int64_t* __restrict__ counts,
+                                              const int64_t* __restrict__ offsets,
+                                              int64_t* __restrict__ oidx,
+                                              double* __restrict__ odist, int want_d2) {
+  __shared__ int32_t sstk[4][kStack];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int64_t gw = (int64_t)blockIdx.x * nw + w;
+  int32_t* stk = gstack ? gstack + gw * stack_len : sstk[w];
+  int64_t slot = gw * 32 + lane;
+  bool valid = slot < nq;
+  int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) q[j] = valid ? Q[qi * D + j] : 0.0;
+  double rr = valid ? r2 : -1.0;
+  int64_t cnt = 0;
+  int64_t cur = (FILL && valid) ? offsets[qi] : 0;
+  const int64_t cur_end = (FILL && valid) ? offsets[qi + 1] : 0;
+  int32_t cov_lo = 0, cov_hi = 0;  // point range already counted whole (count pass)
+  int top = 0;
+  if (lane == 0) stk[0] = 0;
+  __syncwarp();
+  while (top >= 0) {
+    int32_t node = stk[top];
+    --top;
+    __syncwarp();
+    NodeMeta m = load_meta(tv.meta, node);
+    bool need = box_mind2<D, PER>(tv, q, node) <= rr;
+    if (!FILL && need && m.start >= cov_lo && m.start < cov_hi) need = false;
+    if (!FILL && !PER && need && m.left >= 0 && box_maxd2<D>(tv, q, node) <= rr) {
+      cnt += m.count;  // whole subtree inside the ball
+      cov_lo = m.start;
+      cov_hi = m.start + m.count;
+      need = false;
+    }
+    unsigned nm = __ballot_sync(0xffffffffu, need);
+    if (nm == 0) continue;
+    if (m.left < 0) {
+      for (int i = 0; i < m.count; ++i) {
+        int32_t p = m.start + i;
+        double d2 = point_d2<D, PER>(tv, q, p);
+        if (need && d2 <= rr) {
+          if (FILL) {
+            if (cur >= cur_end) continue;  // the row is full (count and fill always agree)
+            oidx[cur] = __ldg(&tv.ids[p]);
+            odist[cur] = want_d2 ? d2 : sqrt(d2);
+            ++cur;
+          } else {
+            ++cnt;
+          }
+        }
+      }
+    } else {
+      if (lane == 0) {
+        stk[top + 1] = m.left + 1;
+        stk[top + 2] = m.left;
+      }
+      top += 2;
+      __syncwarp();
+    }
+  }
+  if (!FILL && valid) counts[qi] = cnt;
+}
+
+// Per-row sort by (d2, id) of the fill output (d2 stored in dist), then sqrt.
+// Insertion sort for short rows, heap sort otherwise.
+__global__ void k_sort_rows(const int64_t* __restrict__ offsets, int64_t nq,
+                            int64_t* __restrict__ idx, double* __restrict__ dist) {
+  int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= nq) return;
+  int64_t b = offsets[qi], e = offsets[qi + 1], n = e - b;
+  double* D2 = dist + b;
+  int64_t* I = idx + b;
+  auto lt = [](double d1, int64_t i1, double d2, int64_t i2) {
+    return d1 < d2 || (d1 == d2 && i1 < i2);
+  };
+  if (n <= 32) {
+    for (int64_t i = 1; i < n; ++i) {
+      double d = D2[i];
+      int64_t x = I[i];
+      int64_t j = i - 1;
+      while (j >= 0 && lt(d, x, D2[j], I[j])) {
+        D2[j + 1] = D2[j];
+        I[j + 1] = I[j];
+        --j;
+      }
+      D2[j + 1] = d;
+      I[j + 1] = x;
+    }
+  } else {
+    auto sift = [&](int64_t i, int64_t end, double d, int64_t x) {
+      for (;;) {
+        int64_t l = 2 * i + 1;
+        if (l >= end) break;
+        int64_t c = l;
+        if (l + 1 < end && lt(D2[l], I[l], D2[l + 1], I[l + 1])) c = l + 1;
+        if (!lt(d, x, D2[c], I[c])) break;
+        D2[i] = D2[c];
+        I[i] = I[c];
+        i = c;
+      }
+      D2[i] = d;
+      I[i] = x;
+    };
+    for (int64_t i = n / 2 - 1; i >= 0; --i) sift(i, n, D2[i], I[i]);
+    for (int64_t end = n - 1; end > 0; --end) {
+      double d = D2[end];
+      int64_t x = I[end];
+      D2[end] = D2[0];
+      I[end] = I[0];
+      sift(0, end, d, x);
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) D2[i] = sqrt(D2[i]);
+}
+
+template <int D, bool FILL>
+__global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restrict__ boxes,
+                                             int64_t nb, int32_t* __restrict__ gstack,
+                                             int stack_len, int64_t* __restrict__ counts,
+                                             const int64_t* __restrict__ offsets,
+                                             int64_t* __restrict__ oidx) {
+  __shared__ int32_t snode[4][kStack];
+  __shared__ unsigned smask[4][kStack];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int64_t gw = (int64_t)blockIdx.x * nw + w;
+  int32_t* stn = gstack ? gstack + gw * 2 * stack_len : snode[w];
+  unsigned* stm = gstack ? reinterpret_cast<unsigned*>(gstack + gw * 2 * stack_len + stack_len)
+                         : smask[w];
+  int64_t bi = gw * 32 + lane;
+  bool valid = bi < nb;
+  double lo[D], hi[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    lo[j] = valid ? boxes[bi * 2 * D + 2 * j] : 0.0;
+    hi[j] = valid ? boxes[bi * 2 * D + 2 * j + 1] : -1.0;
+  }
+  const unsigned bit = 1u << lane;
+  unsigned vm = __ballot_sync(0xffffffffu, valid);
+  int64_t cnt = 0;
+  int64_t cur = (FILL && valid) ? offsets[bi] : 0;
+  const int64_t cur_end = (FILL && valid) ? offsets[bi + 1] : 0;
+  int top = 0;
+  if (lane == 0) {
+    stn[0] = 0;
+    stm[0] = vm;
+  }
+  __syncwarp();
+  while (top >= 0) {
+    int32_t node = stn[top];
+    unsigned mask = stm[top];
+    --top;
+    __syncwarp();
+    bool mine = (mask & bit) != 0;
+    NodeMeta m = load_meta(tv.meta, node);
+    if (m.left < 0) {
+      for (int i = 0; i < m.count; ++i) {
+        int32_t p = m.start + i;
+        bool in = mine;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          double x = __ldg(&tv.pts[(int64_t)j * tv.n + p]);
+          in = in && !(x < lo[j] || x > hi[j]);  // :1319
+        }
+        if (in) {
+          if (FILL) {
+            if (cur < cur_end) oidx[cur++] = __ldg(&tv.ids[p]);
+          } else {
+            ++cnt;
+          }
+        }
+      }
+    } else {
+      double bl = 0.0, bh = 0.0;
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        if (j == m.axis) {
+          bl = lo[j];
+          bh = hi[j];
+        }
+      unsigned lm = __ballot_sync(0xffffffffu, mine && bl < m.split);  // :1296
+      unsigned rm = __ballot_sync(0xffffffffu, mine && bh > m.split);  // :1300
+      if (lane == 0) {
+        int t2 = top;
+        if (rm) {
+          ++t2;
+          stn[t2] = m.left + 1;
+          stm[t2] = rm;
+        }
+        if (lm) {
+          ++t2;
+          stn[t2] = m.left;
+          stm[t2] = lm;
+        }
+      }
+      top += (rm ? 1 : 0) + (lm ? 1 : 0);
+      __syncwarp();
+    }
+  }
+  if (!FILL && valid) counts[bi] = cnt;
+}
+
+template <int D, bool PER>
+ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq,
+                       double r, bool fill, int sorted, int64_t* counts, const int64_t* offsets,
+                       int64_t* idx, double* dist, cudaStream_t s) {
+  TreeView tv = t->view();
+  const int threads = 128, nw = threads / 32;
+  int64_t warps = cdiv(nq, 32);
+  unsigned blocks = (unsigned)cdiv(warps, nw);
+  int stack_len = std::max(kStack, t->depth + 4);
+  int32_t* gstack = nullptr;
+  if (stack_len > kStack)
+    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
+  double r2 = r * r;  // radius**2 (cosmokdtree.f90:1112)
+  if (fill)
+    k_ball<D, PER, true><<<blocks, threads, 0, s>>>(tv, q, order, nq, r2, gstack, stack_len,
+                                                     nullptr, offsets, idx, dist, sorted ? 1 : 0);
+  else
+    k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, r2, gstack, stack_len,
+                                                      counts, nullptr, nullptr, nullptr, 0);
+  CKD_CUDA(cudaGetLastError());
+  if (fill && sorted) {
+    k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist);
+    CKD_CUDA(cudaGetLastError());
+  }
+  if (gstack) CKD_CUDA(dev_free(gstack, s));
+  return CKD_OK;
+}
+
+template <int D>
+ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool fill,
+                      int64_t* counts, const int64_t* offsets, int64_t* idx, cudaStream_t s) {
+  TreeView tv = t->view();
+  const int threads = 128, nw = threads / 32;
+  int64_t warps = cdiv(nb, 32);
+  unsigned blocks = (unsigned)cdiv(warps, nw);
+  int stack_len = std::max(kStack, t->depth + 4);
+  int32_t* gstack = nullptr;
+  if (stack_len > kStack)
+    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw, s));
+  if (fill)
+    k_box<D, true><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, nullptr, offsets,
+                                              idx);
+  else
+    k_box<D, false><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, counts, nullptr,
+                                               nullptr);
+  CKD_CUDA(cudaGetLastError());
+  if (gstack) CKD_CUDA(dev_free(gstack, s));
+  return CKD_OK;
+}
+
+}  // namespace
+
+bool want_order(const ckd_tree* t, int64_t nq);
+
+ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
+                    int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
+                    cudaStream_t s) {
+  int32_t* order = nullptr;
+  if (want_order(t, nq)) {
+    CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
+    CKD_TRY(query_order(t, q, nq, order, s));
+  }
+  ckd_status st;
+#define CKD_BALL_CASE(DD)                                                                      \
+  case DD:                                                                                     \
+    st = t->periodic ? ball_launch<DD, true>(t, q, order, nq, r, fill, sorted, counts, offsets, \
+                                             idx, dist, s)                                     \
+                     : ball_launch<DD, false>(t, q, order, nq, r, fill, sorted, counts,         \
+                                              offsets, idx, dist, s);                          \
+    break;
+  switch (t->d) {
+    CKD_BALL_CASE(1)
+    CKD_BALL_CASE(2)
+    CKD_BALL_CASE(3)
+    CKD_BALL_CASE(4)
+    CKD_BALL_CASE(5)
+    CKD_BALL_CASE(6)
+    CKD_BALL_CASE(7)
+    CKD_BALL_CASE(8)
+    default: st = fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+  }
+#undef CKD_BALL_CASE
+  if (order) dev_free(order, s);
+  return st;
+}
+
+ckd_status box_run(const ckd_tree* t, const double* boxes, int64_t nb, bool fill, int64_t* counts,
+                   const int64_t* offsets, int64_t* idx, cudaStream_t s) {
+  switch (t->d) {
+    case 1: return box_launch<1>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 2: return box_launch<2>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 3: return box_launch<3>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 4: return box_launch<4>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 5: return box_launch<5>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 6: return box_launch<6>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 7: return box_launch<7>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 8: return box_launch<8>(t, boxes, nb, fill, counts, offsets, idx, s);
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+}
+
+}  // namespace ckd

@@ -1,0 +1,153 @@
+// ckd_common.cuh -- shared types and device helpers of libckd (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <cfloat>
+#include <string>
+
+#include "../../include/ckd.h"
+
+#define CKD_MAX_D 8
+
+namespace ckd {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+ckd_status fail(ckd_status st, const std::string& msg);
+ckd_status cuda_fail(cudaError_t e, const char* what);
+
+#define CKD_CUDA(call)                                       \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return ::ckd::cuda_fail(_e, #call); \
+  } while (0)
+
+#define CKD_TRY(call)                    \
+  do {                                   \
+    ckd_status _s = (call);              \
+    if (_s != CKD_OK) return _s;         \
+  } while (0)
+
+// stream-ordered scratch allocation from a per-device pool
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
+cudaError_t dev_free(void* p, cudaStream_t s);
+
+// ------------------------------------------------------------- node layout
+// One 32-byte record per node.  Children of an internal node are allocated as a
+// pair: right = left + 1.  start/count give the node's range in the leaf-ordered
+// point arrays (every subtree is contiguous there).
+struct __align__(16) NodeMeta {
+  double split;   // splitting value (cosmokdtree.f90:412 node%point)
+  int32_t left;   // left child, -1 for a leaf
+  int32_t axis;   // splitting axis, -1 for a leaf
+  int32_t start;  // first leaf-ordered point of the subtree
+  int32_t count;  // number of points in the subtree
+  int32_t depth;  // root = 0
+  int32_t parent; // -1 for the root
+};
+static_assert(sizeof(NodeMeta) == 32, "NodeMeta must be 32 bytes");
+
+// Read-only view of a built tree handed to kernels.
+struct TreeView {
+  int32_t n;
+  int32_t n_nodes;
+  int32_t d;
+  int32_t periodic;
+  double L[CKD_MAX_D];       // box side (periodic)
+  const NodeMeta* meta;      // [n_nodes]
+  const double* box;         // [n_nodes][2d] tight bounding box lo0,hi0,lo1,hi1,...
+  const double* cell;        // [n_nodes][2d] sliding-midpoint cell (reference node bounds)
+  const double* pts;         // SoA [d][n], leaf order
+  const int32_t* ids;        // [n] original index per leaf-ordered point
+};
+
+// --------------------------------------------------------- exact FP64 math
+// Every FP64 product and sum below is separately rounded (explicit _rn
+// intrinsics block FMA contraction), the evaluation order of
+// cosmokdtree.f90:1441-1465 (axis order, d2 = 0 + dx0^2 + dx1^2 + ...).
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
+// minimum image of a coordinate difference: min(|dx|, L - |dx|)  (cosmokdtree.f90:1455)
+__device__ __forceinline__ double min_image(double dx, double L) {
+  double a = fabs(dx);
+  double b = dsub(L, a);
+  return a < b ? a : b;
+}
+
+// Lower bound of the squared distance from q to any point of [lo, hi] on one
+// axis.  Non-periodic: distance to the nearer face (cosmokdtree.f90:1536-1542).
+// Periodic: the nearer of the two faces under the minimum image, which bounds
+// every point of the interval from below (also after rounding, because each
+// rounded operation is monotone in its inputs).
+template <bool PER>
+__device__ __forceinline__ double axis_gap(double x, double lo, double hi, double L) {
+  if (x >= lo && x <= hi) return 0.0;
+  if (!PER) return x < lo ? dsub(lo, x) : dsub(x, hi);
+  double a = min_image(dsub(x, lo), L);
+  double b = min_image(dsub(x, hi), L);
+  return a < b ? a : b;
+}
+
+// ------------------------------------------------------ ordered double keys
+// Monotone map double -> uint64 so that atomicMin/atomicMax on the key order
+// doubles (NaNs sort beyond the infinities).
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+  unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+__host__ __device__ inline unsigned long long dkey_host_pos_inf_min() { return ~0ull; }  // key above any double
+
+// HUGE(0.0) of the reference promoted to FP64 (cosmokdtree.f90:517)
+#define CKD_HUGE ((double)FLT_MAX)
+
+// ------------------------------------------------------------------ misc
+__host__ __device__ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Launch helpers implemented in scan.cu
+// exclusive scan of n int32 values into int64 (out has n+1 entries, out[n] = total)
+ckd_status scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, cudaStream_t s);
+// exclusive scan of n int64 values (out has n+1 entries)
+ckd_status scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+// exclusive scan of n int32 values into int32 (out has n+1 entries)
+ckd_status scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
+
+}  // namespace ckd
+
+// Host-side tree object behind the opaque ckd_tree* handle.
+struct ckd_tree {
+  int device = 0;
+  int64_t n = 0;
+  int d = 0;
+  int leaf = 16;
+  int periodic = 0;
+  int input_dtype = CKD_F64;
+  double L[CKD_MAX_D] = {0};
+  int32_t n_nodes = 0;
+  int32_t n_leaves = 0;
+  int32_t depth = 0;
+  ckd::NodeMeta* meta = nullptr;
+  double* box = nullptr;
+  double* cell = nullptr;
+  double* pts = nullptr;
+  int32_t* ids = nullptr;
+  ckd::TreeView view() const {
+    ckd::TreeView v;
+    v.n = (int32_t)n;
+    v.n_nodes = n_nodes;
+    v.d = d;
+    v.periodic = periodic;
+    for (int j = 0; j < CKD_MAX_D; ++j) v.L[j] = L[j];
+    v.meta = meta;
+    v.box = box;
+    v.cell = cell;
+    v.pts = pts;
+    v.ids = ids;
+    return v;
+  }
+};

@@ -1,0 +1,70 @@
+// ckd_traverse.cuh -- per-lane distance helpers and the query ordering pass.
+#pragma once
+#include "ckd_common.cuh"
+
+namespace ckd {
+
+// Squared distance between the lane's query and leaf-ordered point p
+// (cosmokdtree.f90:1441-1465: dx = p - q, minimum image, d2 = sum dx^2 in axis order).
+template <int D, bool PER>
+__device__ __forceinline__ double point_d2(const TreeView& tv, const double (&q)[D], int32_t p) {
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double dx = dsub(__ldg(&tv.pts[(int64_t)j * tv.n + p]), q[j]);
+    if (PER) dx = min_image(dx, tv.L[j]);
+    s = (j == 0) ? dmul(dx, dx) : dadd(s, dmul(dx, dx));
+  }
+  return s;
+}
+
+// Conservative lower bound of the squared distance from q to any point of the
+// node's tight bounding box.
+template <int D, bool PER>
+__device__ __forceinline__ double box_mind2(const TreeView& tv, const double (&q)[D], int32_t node) {
+  const double* b = tv.box + (int64_t)node * 2 * D;
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double g = axis_gap<PER>(q[j], __ldg(&b[2 * j]), __ldg(&b[2 * j + 1]), tv.L[j]);
+    s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
+  }
+  return s;
+}
+
+// Upper bound of the squared distance from q to any point of the box
+// (non-periodic; per axis max(|q-lo|, |q-hi|), cosmokdtree.f90:1509-1510).
+template <int D>
+__device__ __forceinline__ double box_maxd2(const TreeView& tv, const double (&q)[D], int32_t node) {
+  const double* b = tv.box + (int64_t)node * 2 * D;
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double a = fabs(dsub(q[j], __ldg(&b[2 * j])));
+    double c = fabs(dsub(q[j], __ldg(&b[2 * j + 1])));
+    double g = a > c ? a : c;
+    s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
+  }
+  return s;
+}
+
+__device__ __forceinline__ NodeMeta load_meta(const NodeMeta* m, int32_t node) {
+  const int4* p = reinterpret_cast<const int4*>(m + node);
+  int4 a = __ldg(p), b = __ldg(p + 1);
+  NodeMeta r;
+  r.split = __hiloint2double(a.y, a.x);
+  r.left = a.z;
+  r.axis = a.w;
+  r.start = b.x;
+  r.count = b.y;
+  r.depth = b.z;
+  r.parent = b.w;
+  return r;
+}
+
+// Order queries by the leaf they fall in (a counting sort on the leaf's first
+// point), so that the 32 lanes of a warp hold spatially adjacent queries.
+ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
+                       cudaStream_t s);
+
+}  // namespace ckd

@@ -1,0 +1,300 @@
+"""Drop-in replacement of cosmokdtree's Python API (src/cosmokdtree/kdtree.py:16-87).
+
+Same functions, arguments, defaults and results as the reference:
+
+* ``build_kdtree(points, leaf=None, boxsize=None)``      (kdtree.py:16-34)
+* ``deallocate_kdtree(tree)``                              (kdtree.py:37-38)
+* ``knn_search(tree, target, k, sorted=True)``             (kdtree.py:41-53)
+* ``ball_search(tree, target, radius, sorted=False)``      (kdtree.py:56-79)
+* ``box_search(tree, box)``                                (kdtree.py:82-87)
+
+plus batched variants that keep results on the GPU:
+
+* ``knn_search_batch``  -> (dist, idx) CUDA tensors of shape (nq, k)
+* ``ball_search_csr``   -> (offsets, idx, dist) CSR CUDA tensors
+* ``box_search_csr``    -> (offsets, idx) CSR CUDA tensors for many boxes
+
+Every search runs on the B200 through libckd.so (include/ckd.h); there is no CPU
+path.  Host (numpy) inputs are copied to the device and results copied back;
+CUDA-tensor inputs stay on the device.  Ids are 0-based int64; a kNN slot with no
+neighbour (k > n) holds id -2 and distance 1.8446743523953730e19 exactly as the
+reference returns them.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import CKDArgumentError, check
+
+__all__ = [
+    "KDTree", "build_kdtree", "deallocate_kdtree", "knn_search", "ball_search", "box_search",
+    "knn_search_batch", "ball_search_csr", "box_search_csr",
+]
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class KDTree:
+    """Opaque handle of a tree built on the GPU (the reference returns an int64 address,
+    src/cosmokdtree2py.f90:70-73)."""
+
+    def __init__(self, handle, n, d, leaf, boxsize, device):
+        self._h = handle
+        self.n = n
+        self.d = d
+        self.leaf = leaf
+        self.boxsize = boxsize
+        self.periodic = boxsize is not None
+        self.device = device
+        info = [ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()]
+        check(_lib.load().ckd_tree_info(self._h, None, None, None, None, ctypes.byref(info[0]),
+                                        ctypes.byref(info[1]), ctypes.byref(info[2]), None))
+        self.n_nodes, self.n_leaves, self.depth = (int(x.value) for x in info)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "tree has been deallocated")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.load().ckd_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export(self) -> dict:
+        """Structure in preorder (left first): axis (-1 leaf), split, start, count,
+        left/right preorder children, cell and tight box (n_nodes x 2d), ids (leaf order)."""
+        m, d = self.n_nodes, self.d
+        out = dict(axis=np.empty(m, np.int32), split=np.empty(m), start=np.empty(m, np.int64),
+                   count=np.empty(m, np.int64), left=np.empty(m, np.int64),
+                   right=np.empty(m, np.int64), cell=np.empty((m, 2 * d)),
+                   box=np.empty((m, 2 * d)), ids=np.empty(self.n, np.int64))
+        P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
+        with torch.cuda.device(self.device):
+            check(_lib.load().ckd_tree_export(
+                self.handle, P(out["axis"], ctypes.c_int32), P(out["split"], ctypes.c_double),
+                P(out["start"], ctypes.c_int64), P(out["count"], ctypes.c_int64),
+                P(out["left"], ctypes.c_int64), P(out["right"], ctypes.c_int64),
+                P(out["cell"], ctypes.c_double), P(out["box"], ctypes.c_double),
+                P(out["ids"], ctypes.c_int64)))
+        return out
+
+
+# ---------------------------------------------------------------- helpers
+
+def _on_device(x) -> bool:
+    return isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def _queries(tree: KDTree, target) -> tuple[torch.Tensor, bool]:
+    """(nq, d) contiguous FP64 CUDA tensor on the tree's device, and whether the
+    caller passed device data.  A 1-D target is one point (kdtree.py:45-46)."""
+    dev = _on_device(target)
+    if dev:
+        q = target.to(device=f"cuda:{tree.device}", dtype=torch.float64)
+    else:
+        q = torch.from_numpy(np.array(target, dtype=np.float64, copy=True, ndmin=1))
+    if q.dim() == 1:
+        q = q.reshape(1, -1)
+    if q.dim() != 2 or q.shape[1] != tree.d:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
+                               "target dimensionality does not match the tree")
+    if tree.periodic and q.shape[0] > 0:
+        half = torch.as_tensor(tree.boxsize / 2.0, dtype=torch.float64, device=q.device)
+        bad = (q < -half) | (q > half) | torch.isnan(q)
+        if bool(bad.any()):
+            raise CKDArgumentError(_lib.CKD_ERR_OUT_OF_BOX,
+                                   "periodic tree: query points must lie in [-L/2, L/2]")
+    if not dev:
+        q = q.pin_memory().to(f"cuda:{tree.device}", non_blocking=True)
+    return q.contiguous(), dev
+
+
+def _to_host(t: torch.Tensor) -> np.ndarray:
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return h.numpy()
+
+
+# ---------------------------------------------------------------- build
+
+def build_kdtree(points, leaf=None, boxsize=None) -> KDTree:
+    """Build a k-d tree (kdtree.py:16-34).  ``boxsize=None`` gives a non-periodic tree;
+    otherwise the tree is periodic with box sides ``boxsize`` and every coordinate must
+    lie in [-L/2, L/2] (cosmokdtree.f90:177-190).  FP32 input is kept FP32 on the copy
+    and widened on the device."""
+    if leaf is None:
+        leaf = 16
+    if not (int(leaf) == leaf and leaf > 0):
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "Leaf size must be a positive integer")
+    leaf = int(leaf)
+    dev_in = _on_device(points)
+    if dev_in:
+        pts = points
+        if pts.dtype not in (torch.float32, torch.float64):
+            pts = pts.to(torch.float64)
+    else:
+        arr = np.asarray(points)
+        if arr.dtype != np.float32:
+            arr = arr.astype(np.float64, copy=False)
+        pts = torch.from_numpy(np.ascontiguousarray(arr))
+    if pts.dim() != 2:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM, "points must be an (n, d) array")
+    n, d = pts.shape
+    box = None
+    if boxsize is not None:
+        if np.ndim(boxsize) == 0:  # a scalar side is broadcast to every axis
+            boxsize = np.full(d, float(boxsize))
+        box = np.array(boxsize, dtype=np.float64, ndmin=1)
+        if len(box) != d:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
+                                   "Incorrect dimensions for boxsize var. Size must be [Lx, Ly, Lz, ...]")
+        if np.all(box == -1.0):  # the reference's "not periodic" sentinel (cosmokdtree2py.f90:48-55)
+            box = None
+    dtype = _lib.CKD_F32 if pts.dtype == torch.float32 else _lib.CKD_F64
+    if dev_in:
+        device = pts.device.index if pts.device.index is not None else torch.cuda.current_device()
+    else:
+        device = torch.cuda.current_device()
+    with torch.cuda.device(device):
+        if not dev_in:
+            pts = pts.pin_memory().to(f"cuda:{device}", non_blocking=True)
+        pts = pts.contiguous()
+        h = ctypes.c_void_p()
+        boxp = box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if box is not None else None
+        check(_lib.load().ckd_build(_ptr(pts), n, d, dtype, leaf, boxp, 1, _stream(),
+                                    ctypes.byref(h)))
+    return KDTree(h, n, d, leaf, box, device)
+
+
+def deallocate_kdtree(tree: KDTree) -> None:
+    """Free the tree's device memory (kdtree.py:37-38)."""
+    tree.close()
+
+
+# ---------------------------------------------------------------- kNN
+
+def _check_k(k):
+    if type(k) not in (int, np.int32, np.int64):  # kdtree.py:42
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be an integer")
+    if k < 1:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be a positive integer")
+    return int(k)
+
+
+def knn_search_batch(tree: KDTree, target, k, sorted=True):
+    """k nearest neighbours of every target point; (dist, idx) CUDA tensors (nq, k)."""
+    k = _check_k(k)
+    with torch.cuda.device(tree.device):
+        q, _ = _queries(tree, target)
+        nq = q.shape[0]
+        dist = torch.empty((nq, k), dtype=torch.float64, device=q.device)
+        idx = torch.empty((nq, k), dtype=torch.int64, device=q.device)
+        check(_lib.load().ckd_knn(tree.handle, _ptr(q), nq, k, int(bool(sorted)), _ptr(dist),
+                                  _ptr(idx), _stream()))
+    return dist, idx
+
+
+def knn_search(tree: KDTree, target, k, sorted=True):
+    """k nearest neighbours (kdtree.py:41-53).  Returns (dist, idx), each (ntar, k):
+    numpy arrays for host input, CUDA tensors for CUDA-tensor input."""
+    dist, idx = knn_search_batch(tree, target, k, sorted)
+    if _on_device(target):
+        return dist, idx
+    with torch.cuda.device(tree.device):
+        return _to_host(dist), _to_host(idx)
+
+
+# ---------------------------------------------------------------- ball
+
+def _check_radius(radius):
+    if not radius > 0.0:  # kdtree.py:57
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "Radius must be a positive number")
+    return float(radius)
+
+
+def ball_search_csr(tree: KDTree, target, radius, sorted=False):
+    """All points within ``radius`` of every target, as CSR CUDA tensors
+    (offsets (nq+1,), idx, dist)."""
+    radius = _check_radius(radius)
+    L = _lib.load()
+    with torch.cuda.device(tree.device):
+        q, _ = _queries(tree, target)
+        nq = q.shape[0]
+        counts = torch.empty(nq, dtype=torch.int64, device=q.device)
+        offsets = torch.zeros(nq + 1, dtype=torch.int64, device=q.device)
+        if nq > 0:
+            check(L.ckd_ball_count(tree.handle, _ptr(q), nq, radius, _ptr(counts), _stream()))
+            check(L.ckd_exclusive_scan(_ptr(counts), _ptr(offsets), nq, _stream()))
+        total = int(offsets[-1].item())
+        idx = torch.empty(total, dtype=torch.int64, device=q.device)
+        dist = torch.empty(total, dtype=torch.float64, device=q.device)
+        if nq > 0 and total > 0:
+            check(L.ckd_ball_fill(tree.handle, _ptr(q), nq, radius, int(bool(sorted)),
+                                  _ptr(offsets), _ptr(idx), _ptr(dist), _stream()))
+    return offsets, idx, dist
+
+
+def ball_search(tree: KDTree, target, radius, sorted=False):
+    """Ball search (kdtree.py:56-79): per target lists of distances and 0-based ids."""
+    offsets, idx, dist = ball_search_csr(tree, target, radius, sorted)
+    with torch.cuda.device(tree.device):
+        off, i, d = _to_host(offsets), _to_host(idx), _to_host(dist)
+    n = len(off) - 1
+    return ([d[off[j]:off[j + 1]] for j in range(n)], [i[off[j]:off[j + 1]] for j in range(n)])
+
+
+# ---------------------------------------------------------------- box
+
+def box_search_csr(tree: KDTree, boxes):
+    """Points inside each of many axis-aligned boxes ([lo0, hi0, lo1, hi1, ...] rows),
+    CSR CUDA tensors (offsets (nb+1,), idx)."""
+    L = _lib.load()
+    with torch.cuda.device(tree.device):
+        if _on_device(boxes):
+            b = boxes.to(device=f"cuda:{tree.device}", dtype=torch.float64)
+        else:
+            b = torch.from_numpy(np.array(boxes, dtype=np.float64, copy=True, ndmin=1))
+        if b.dim() == 1:
+            b = b.reshape(1, -1)
+        if b.shape[-1] != 2 * tree.d:  # cosmokdtree2py.f90:275-277
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
+                                   "Error: box size does not match tree dimensionality.")
+        b = b.to(f"cuda:{tree.device}").contiguous()
+        nb = b.shape[0]
+        counts = torch.empty(nb, dtype=torch.int64, device=b.device)
+        offsets = torch.zeros(nb + 1, dtype=torch.int64, device=b.device)
+        if nb > 0:
+            check(L.ckd_box_count(tree.handle, _ptr(b), nb, _ptr(counts), _stream()))
+            check(L.ckd_exclusive_scan(_ptr(counts), _ptr(offsets), nb, _stream()))
+        total = int(offsets[-1].item())
+        idx = torch.empty(total, dtype=torch.int64, device=b.device)
+        if nb > 0 and total > 0:
+            check(L.ckd_box_fill(tree.handle, _ptr(b), nb, _ptr(offsets), _ptr(idx), _stream()))
+    return offsets, idx
+
+
+def box_search(tree: KDTree, box):
+    """Ids of the points inside one box [xmin, xmax, ymin, ymax, ...] (kdtree.py:82-87)."""
+    b = np.array(box, dtype=np.float64, ndmin=1).reshape(-1)
+    offsets, idx = box_search_csr(tree, b.reshape(1, -1))
+    with torch.cuda.device(tree.device):
+        return _to_host(idx)

@@ -1,0 +1,116 @@
+/* ckd.h -- C ABI of libckd, the B200 (sm_100a) k-d tree library.
+ *
+ * Drop-in boundary for cosmokdtree's build_kdtree / knn_search / ball_search /
+ * box_search path.  Every entry point is extern "C", takes plain pointers and
+ * sizes, returns a ckd_status and never aborts the process (the reference STOPs:
+ * src/cosmokdtree.f90:161,170,190; src/cosmokdtree2py.f90:58,276).  On failure
+ * ckd_last_error() returns a message for the calling thread.
+ *
+ * Pointers suffixed _dev are device pointers on the tree's device; _host
+ * variants take host memory and do the copies themselves.  `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  Device-pointer
+ * calls are asynchronous on `stream` unless stated otherwise.
+ *
+ * Ids are 0-based int64 (the reference returns 1-based ids that
+ * src/cosmokdtree/kdtree.py:52,75,86 shift with `idx -= 1`).  A kNN slot with no
+ * neighbour (k > n) holds id -2 and distance sqrt(FLT_MAX) = 1.8446743523953730e19,
+ * the values the reference's Python API returns.
+ */
+#ifndef CKD_H_
+#define CKD_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ckd_status {
+  CKD_OK = 0,
+  CKD_ERR_BAD_DIM = 1,     /* dimensionality mismatch / unsupported D */
+  CKD_ERR_OUT_OF_BOX = 2,  /* periodic: coordinate outside [-L/2, L/2] */
+  CKD_ERR_BAD_ARG = 3,     /* null pointer, k <= 0, radius <= 0, n < 1, NaN, ... */
+  CKD_ERR_OOM = 4,         /* device allocation failed */
+  CKD_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+  CKD_ERR_CUDA = 6,        /* any other CUDA runtime error */
+  CKD_ERR_NO_DEVICE = 7,   /* no usable sm_100 device */
+  CKD_ERR_DEPTH = 8        /* tree deeper than the build's level cap */
+} ckd_status;
+
+typedef enum ckd_dtype { CKD_F64 = 0, CKD_F32 = 1 } ckd_dtype;
+
+typedef struct ckd_tree ckd_tree; /* opaque handle owning all device buffers */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ckd_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ckd_last_error(void);
+
+/* Build a tree.
+ * Replaces pybuild_kdtree (src/cosmokdtree2py.f90:29-74) / build_kdtree
+ * (src/cosmokdtree.f90:124-238).
+ * pts: n x d row-major, dtype CKD_F64 or CKD_F32 (FP32 input is widened to FP64).
+ * pts_on_device: 1 if pts is a device pointer, 0 if host memory.
+ * leaf: leaf size (reference default 16).  boxsize: d box sides for a periodic
+ * tree (coordinates must lie in [-L/2, L/2]), or NULL for a non-periodic tree.
+ * Synchronises `stream` before returning. */
+ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf,
+                     const double* boxsize, int pts_on_device, void* stream, ckd_tree** out);
+
+/* Free a tree and its device buffers (replaces pydeallocate_tree,
+ * src/cosmokdtree2py.f90:80-97).  NULL is accepted. */
+ckd_status ckd_free(ckd_tree* tree);
+
+/* Scalar properties of a built tree.  Any output pointer may be NULL. */
+ckd_status ckd_tree_info(const ckd_tree* tree, int64_t* n, int* d, int* leaf, int* periodic,
+                         int32_t* n_nodes, int32_t* n_leaves, int32_t* depth, int* device);
+
+/* Copy the tree structure to host memory, nodes in preorder (left subtree first),
+ * for structural comparison.  Each output may be NULL; sizes are n_nodes (per
+ * node), n_nodes*2*d (cell, box) and n (ids, leaf order).  axis = -1 marks a leaf.
+ * left/right are preorder indices (-1 for leaves).  Synchronous. */
+ckd_status ckd_tree_export(const ckd_tree* tree, int32_t* axis, double* split, int64_t* start,
+                           int64_t* count, int64_t* left, int64_t* right, double* cell,
+                           double* box, int64_t* ids);
+
+/* Exact k nearest neighbours of nq query points (row-major nq x d FP64).
+ * Replaces pyknn_search (src/cosmokdtree2py.f90:103-143) / knn_search
+ * (src/cosmokdtree.f90:504-540).  Results ranked by (squared distance, id);
+ * dist_dev / idx_dev are nq x k row-major.  sorted=0 allows any order inside a row. */
+ckd_status ckd_knn(const ckd_tree* tree, const double* q_dev, int64_t nq, int k, int sorted,
+                   double* dist_dev, int64_t* idx_dev, void* stream);
+
+/* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
+ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
+                        double* dist_host, int64_t* idx_host, void* stream);
+
+/* Ball search, two-phase CSR protocol.  Replaces pyball_search_call_1/2
+ * (src/cosmokdtree2py.f90:153-246) / ball_search (src/cosmokdtree.f90:1015-1212).
+ * Phase 1 writes counts_dev[nq] = number of points with d^2 <= radius^2.
+ * The caller builds offsets_dev[nq+1] (exclusive prefix; ckd_exclusive_scan helps)
+ * and allocates idx/dist of offsets[nq] entries; phase 2 fills them.  sorted=1
+ * orders each row by (squared distance, id); sorted=0 keeps traversal order. */
+ckd_status ckd_ball_count(const ckd_tree* tree, const double* q_dev, int64_t nq, double radius,
+                          int64_t* counts_dev, void* stream);
+ckd_status ckd_ball_fill(const ckd_tree* tree, const double* q_dev, int64_t nq, double radius,
+                         int sorted, const int64_t* offsets_dev, int64_t* idx_dev,
+                         double* dist_dev, void* stream);
+
+/* Box search, two-phase CSR protocol.  Boxes are nb x 2d row-major
+ * [lo0, hi0, lo1, hi1, ...].  Replaces pybox_search_call_1/2
+ * (src/cosmokdtree2py.f90:252-315) / box_search (src/cosmokdtree.f90:1220-1328),
+ * batched over nb boxes.  Descent and inclusion rules are the reference's. */
+ckd_status ckd_box_count(const ckd_tree* tree, const double* boxes_dev, int64_t nb,
+                         int64_t* counts_dev, void* stream);
+ckd_status ckd_box_fill(const ckd_tree* tree, const double* boxes_dev, int64_t nb,
+                        const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
+
+/* out_dev[0] = 0, out_dev[i+1] = in_dev[0] + ... + in_dev[i]  (n+1 outputs). */
+ckd_status ckd_exclusive_scan(const int64_t* in_dev, int64_t* out_dev, int64_t n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CKD_H_ */
