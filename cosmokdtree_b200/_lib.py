@@ -78,13 +78,16 @@ SIGNATURES = {
     "ckd_tree_export": [_vp, _pi32, _pdbl, _pi64, _pi64, _pi64, _pi64, _pdbl, _pdbl, _pi64],
     "ckd_knn": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
     "ckd_knn_host": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
+    "ckd_query_order": [_vp, _vp, _i64, _vp, _vp],
+    "ckd_knn_ordered": [_vp, _vp, _i64, _vp, _int, _int, _vp, _vp, _vp],
+    "ckd_launch_count": [],
     "ckd_ball_count": [_vp, _vp, _i64, _dbl, _vp, _vp],
     "ckd_ball_fill": [_vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],
     "ckd_box_fill": [_vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_exclusive_scan": [_vp, _vp, _i64, _vp],
 }
-_RESTYPES = {"ckd_last_error": ctypes.c_char_p}
+_RESTYPES = {"ckd_last_error": ctypes.c_char_p, "ckd_launch_count": ctypes.c_int64}
 
 
 def load(path: str = LIB_PATH):

@@ -1,4 +1,5 @@
 // api.cu -- the extern "C" boundary of libckd (declared in include/ckd.h).
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -26,6 +27,9 @@ ckd_status cuda_fail(cudaError_t e, const char* what) {
     return CKD_ERR_NO_DEVICE;
   return CKD_ERR_CUDA;
 }
+
+static std::atomic<int64_t> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ---------------------------------------------------------- scratch memory
 // One stream-ordered pool per device, keeping freed blocks cached.
@@ -68,6 +72,10 @@ cudaError_t dev_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) :
 ckd_status build_dispatch(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t s);
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s);
+ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, cudaStream_t s);
+ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
+                       cudaStream_t s);
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s);
@@ -243,6 +251,27 @@ ckd_status ckd_knn(const ckd_tree* t, const double* q, int64_t nq, int k, int so
   if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
   return knn_run(t, q, nq, k, sorted, dist, idx, (cudaStream_t)stream);
 }
+
+ckd_status ckd_query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
+                           void* stream) {
+  CKD_TRY(check_tree(t));
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !order) return fail(CKD_ERR_BAD_ARG, "null query or order pointer");
+  return query_order(t, q, nq, order, (cudaStream_t)stream);
+}
+
+ckd_status ckd_knn_ordered(const ckd_tree* t, const double* q, int64_t nq, const int32_t* order,
+                           int k, int sorted, double* dist, int64_t* idx, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  return knn_ordered(t, q, order, nq, k, sorted, dist, idx, (cudaStream_t)stream);
+}
+
+int64_t ckd_launch_count(void) { return g_launches.load(); }
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                         double* dist, int64_t* idx, void* stream) {

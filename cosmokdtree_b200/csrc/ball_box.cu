@@ -250,10 +250,10 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
   else
     k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, r2, gstack, stack_len,
                                                       counts, nullptr, nullptr, nullptr, 0);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   if (fill && sorted) {
     k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
   }
   if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
@@ -276,7 +276,7 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
   else
     k_box<D, false><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, counts, nullptr,
                                                nullptr);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
 }

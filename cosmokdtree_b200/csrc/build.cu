@@ -550,13 +550,13 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     else
       k_init_points<double><<<g, 256, 0, s>>>((const double*)pts_dev, n, D, B.X[0], B.I[0],
                                               B.NID[0], B.NID[1]);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
   }
   double* Ldev = nullptr;
   CKD_CUDA(dev_alloc((void**)&Ldev, sizeof(double) * CKD_MAX_D, s));
   CKD_CUDA(cudaMemcpyAsync(Ldev, t->L, sizeof(double) * CKD_MAX_D, cudaMemcpyHostToDevice, s));
   k_root_init<D><<<1, 1, 0, s>>>(B.meta, B.cell, B.keys, (int32_t)n, Ldev, t->periodic);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   int32_t root = 0;
   CKD_CUDA(cudaMemcpyAsync(B.act[0], &root, sizeof(int32_t), cudaMemcpyHostToDevice, s));
 
@@ -564,7 +564,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   // non-periodic root cell.  Computed with the open-node reduction using a leaf
   // threshold of 0 so that the root is always "open" here.
   k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], B.meta, 0, 0, n, B.keys);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   unsigned long long rk[2 * CKD_MAX_D];
   CKD_CUDA(cudaMemcpyAsync(rk, B.keys, sizeof(unsigned long long) * 2 * D, cudaMemcpyDeviceToHost, s));
   CKD_CUDA(cudaStreamSynchronize(s));
@@ -613,29 +613,29 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     if (level > 0) {
       k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, level, leaf, n,
                                                     B.keys);
-      CKD_CUDA(cudaGetLastError());
+      CKD_LAUNCH_CHECK();
     }
     k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext,
                                    level == 0 ? root_from_box : 0);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     k_argext<<<(unsigned)cdiv(n, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, level,
                                                     leaf, n, B.ext);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     k_flags<<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, level,
                                              leaf, n, B.tile_sum, B.pstart, B.pend);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntiles, s));
     k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off,
                                      B.nleft, B.pbase, B.keys, n_nodes, leaf, B.nxt_cnt,
                                      B.scal + 1);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.nxt_cnt, B.nxt_off, m, s));
     k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.act[1 - cur]);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     k_scatter<D><<<(unsigned)ntiles, kBT, 0, s>>>(
         B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext, B.tile_off, B.nleft, B.pbase,
         level, leaf, n, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     int32_t nm = 0;
     CKD_CUDA(cudaMemcpyAsync(&nm, B.nxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
@@ -650,7 +650,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
 
   k_leaf_box<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(B.meta, n_nodes, leaf, t->pts, n,
                                                              B.box);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   t->n_nodes = n_nodes;
   t->depth = level;
   CKD_CUDA(cudaMalloc((void**)&t->meta, sizeof(NodeMeta) * n_nodes));

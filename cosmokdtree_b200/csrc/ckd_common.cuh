@@ -22,6 +22,14 @@ ckd_status cuda_fail(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return ::ckd::cuda_fail(_e, #call); \
   } while (0)
 
+// every kernel launch is followed by this: counts the launch, reports launch errors
+void note_launch();
+#define CKD_LAUNCH_CHECK()                 \
+  do {                                     \
+    ::ckd::note_launch();                  \
+    CKD_CUDA(cudaGetLastError());          \
+  } while (0)
+
 #define CKD_TRY(call)                    \
   do {                                   \
     ckd_status _s = (call);              \

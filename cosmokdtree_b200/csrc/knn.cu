@@ -299,7 +299,7 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order, 
     k_knn_rows<D, PER><<<blocks, threads, 0, s>>>(tv, q, order, nq, k, sorted, gstack, stack_len,
                                                   dist, idx);
   }
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
 }
@@ -322,11 +322,11 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   unsigned g = (unsigned)cdiv(nq, 256);
   k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   CKD_TRY(scan_i32(hist, off, n, s));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   k_bucket_scatter<<<g, 256, 0, s>>>(key, nq, off, hist, order);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   CKD_CUDA(dev_free(key, s));
   CKD_CUDA(dev_free(hist, s));
   CKD_CUDA(dev_free(off, s));
@@ -353,6 +353,21 @@ ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* 
 // Queries are ordered by leaf when there are enough of them to fill many warps.
 bool want_order(const ckd_tree* t, int64_t nq) { return nq >= 4096 && nq * 8 >= t->n / 64; }
 
+ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+  switch (t->d) {
+    case 1: return knn_dispatch_d<1>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 2: return knn_dispatch_d<2>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 3: return knn_dispatch_d<3>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 4: return knn_dispatch_d<4>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 5: return knn_dispatch_d<5>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 6: return knn_dispatch_d<6>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 7: return knn_dispatch_d<7>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 8: return knn_dispatch_d<8>(t, q, order, nq, k, sorted, dist, idx, s);
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+}
+
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s) {
   int32_t* order = nullptr;
@@ -360,18 +375,7 @@ ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int so
     CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
     CKD_TRY(query_order(t, q, nq, order, s));
   }
-  ckd_status st;
-  switch (t->d) {
-    case 1: st = knn_dispatch_d<1>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 2: st = knn_dispatch_d<2>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 3: st = knn_dispatch_d<3>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 4: st = knn_dispatch_d<4>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 5: st = knn_dispatch_d<5>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 6: st = knn_dispatch_d<6>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 7: st = knn_dispatch_d<7>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    case 8: st = knn_dispatch_d<8>(t, q, order, nq, k, sorted, dist, idx, s); break;
-    default: st = fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
-  }
+  ckd_status st = knn_ordered(t, q, order, nq, k, sorted, dist, idx, s);
   if (order) dev_free(order, s);
   return st;
 }

@@ -63,7 +63,7 @@ ckd_status scan_impl(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
   int64_t tiles = cdiv(n, kTile);
   if (tiles == 1) {
     k_tile_scan<Tin, Tout><<<1, kThreads, 0, s>>>(in, n, (const Tout*)nullptr, out);
-    CKD_CUDA(cudaGetLastError());
+    CKD_LAUNCH_CHECK();
     return CKD_OK;
   }
   Tout* part = nullptr;
@@ -71,11 +71,11 @@ ckd_status scan_impl(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
   CKD_CUDA(dev_alloc((void**)&part, sizeof(Tout) * tiles, s));
   CKD_CUDA(dev_alloc((void**)&poff, sizeof(Tout) * (tiles + 1), s));
   k_tile_reduce<Tin, Tout><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, part);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   ckd_status st = scan_impl<Tout, Tout>(part, poff, tiles, s);
   if (st != CKD_OK) return st;
   k_tile_scan<Tin, Tout><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, poff, out);
-  CKD_CUDA(cudaGetLastError());
+  CKD_LAUNCH_CHECK();
   CKD_CUDA(dev_free(part, s));
   CKD_CUDA(dev_free(poff, s));
   return CKD_OK;

@@ -110,7 +110,8 @@ def _queries(tree: KDTree, target) -> tuple[torch.Tensor, bool]:
     if dev:
         q = target.to(device=f"cuda:{tree.device}", dtype=torch.float64)
     else:
-        q = torch.from_numpy(np.array(target, dtype=np.float64, copy=True, ndmin=1))
+        q = torch.from_numpy(np.ascontiguousarray(np.array(target, dtype=np.float64, copy=False,
+                                                           ndmin=1)))
     if q.dim() == 1:
         q = q.reshape(1, -1)
     if q.dim() != 2 or q.shape[1] != tree.d:

@@ -81,6 +81,21 @@ ckd_status ckd_tree_export(const ckd_tree* tree, int32_t* axis, double* split, i
 ckd_status ckd_knn(const ckd_tree* tree, const double* q_dev, int64_t nq, int k, int sorted,
                    double* dist_dev, int64_t* idx_dev, void* stream);
 
+/* The two stages of ckd_knn, for callers that reuse a query order or time the
+ * search kernel alone.  No reference counterpart (the reference has no query
+ * ordering).  ckd_query_order writes order_dev[nq]: a permutation of 0..nq-1 that
+ * groups queries by the leaf containing them.  ckd_knn_ordered runs the search in
+ * that order (order_dev may be NULL for input order); results still land in the
+ * queries' own rows. */
+ckd_status ckd_query_order(const ckd_tree* tree, const double* q_dev, int64_t nq,
+                           int32_t* order_dev, void* stream);
+ckd_status ckd_knn_ordered(const ckd_tree* tree, const double* q_dev, int64_t nq,
+                           const int32_t* order_dev, int k, int sorted, double* dist_dev,
+                           int64_t* idx_dev, void* stream);
+
+/* Number of CUDA kernels this library has launched in this process. */
+int64_t ckd_launch_count(void);
+
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);
