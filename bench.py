@@ -37,6 +37,7 @@ WORKLOADS = {
     # name: (n_points, k, periodic, leaf, seed)
     "clustered_periodic_2p24_k32": (1 << 24, 32, True, 16, 1),
     "uniform_2p20_k16": (1 << 20, 16, False, 16, 0),
+    "clustered_periodic_2p22_k32": (1 << 22, 32, True, 16, 1),
 }
 DEFAULT_WORKLOAD = "clustered_periodic_2p24_k32"
 
@@ -188,6 +189,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--variant", type=int, default=0, help="kNN kernel: 0 auto, 1 fp64, 2 screened")
+    ap.add_argument("--stats", action="store_true", help="report traversal statistics (profile mode)")
+    ap.add_argument("--tune", default="", help="comma list key=value of ckd_set_tuning knobs")
+    ap.add_argument("--profile", action="store_true",
+                    help="one build and the kNN steps only (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -217,6 +223,10 @@ def main():
 
     from cosmokdtree_b200 import _lib, kdtree
     L = _lib.load()
+    _lib.check(L.ckd_set_knn_variant(args.variant))
+    for kv in filter(None, args.tune.split(",")):
+        key, val = kv.split("=")
+        _lib.check(L.ckd_set_tuning(int(key), int(val)))
     name = args.workload
     n, k, periodic, leaf, seed = WORKLOADS[name]
     P = make_points(name, seed_offset=rank)
@@ -227,7 +237,8 @@ def main():
     # ---- build (device-resident input), Mpt/s
     Pd = torch.from_numpy(P).cuda()
     build_ms = []
-    for it in range(3):
+    n_builds = 1 if args.profile else 3
+    for it in range(n_builds):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -235,9 +246,9 @@ def main():
         tree = kdtree.build_kdtree(Pd, leaf=leaf, boxsize=box)
         e1.record(stream)
         torch.cuda.synchronize()
-        if it > 0:
+        if it > 0 or n_builds == 1:
             build_ms.append(e0.elapsed_time(e1))
-        if it < 2:
+        if it < n_builds - 1:
             tree.close()
     build_ms_v = allmax(float(np.mean(build_ms)))
 
@@ -266,6 +277,8 @@ def main():
         step()
     torch.cuda.synchronize()
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    if args.stats:
+        _lib.check(L.ckd_knn_stats(1, None))
     launches0 = L.ckd_launch_count()
     with ClockSampler(local) as clk:
         barrier()
@@ -285,6 +298,24 @@ def main():
     ms_per_step = total_ms / args.steps
     value = world * nq * args.steps / (total_ms / 1e3)
     clocks = clk.summary()
+    stats = None
+    if args.stats:
+        st = (ctypes.c_int64 * 8)()
+        _lib.check(L.ckd_knn_stats(0, st))
+        names = ["pops", "needed_pops", "leaf_visits", "points_screened", "insert_rounds",
+                 "fp64_evals", "inserts", "lanes_on_leaf_visits"]
+        warps = args.steps * ((nq + 31) // 32)
+        stats = {nm: st[i] / warps for i, nm in enumerate(names)}
+        stats["per_query_fp64_evals"] = st[5] / (args.steps * nq)
+        stats["per_query_inserts"] = st[6] / (args.steps * nq)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "workload": name, "ms_per_step": ms_per_step,
+                              "variant": args.variant, "tune": args.tune, "stats_per_warp": stats,
+                              "knn_ms": float(np.mean(knn_ms)), "order_ms": float(np.mean(order_ms)),
+                              "build_ms": build_ms_v, "depth": tree.depth, "n_nodes": tree.n_nodes}))
+        tree.close()
+        return 0
 
     # ---- end to end through the public API with host buffers
     e2e_ms = []

@@ -81,6 +81,9 @@ SIGNATURES = {
     "ckd_query_order": [_vp, _vp, _i64, _vp, _vp],
     "ckd_knn_ordered": [_vp, _vp, _i64, _vp, _int, _int, _vp, _vp, _vp],
     "ckd_launch_count": [],
+    "ckd_set_knn_variant": [_int],
+    "ckd_set_tuning": [_int, _int],
+    "ckd_knn_stats": [_int, _pi64],
     "ckd_ball_count": [_vp, _vp, _i64, _dbl, _vp, _vp],
     "ckd_ball_fill": [_vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],

@@ -29,6 +29,11 @@ ckd_status cuda_fail(cudaError_t e, const char* what) {
 }
 
 static std::atomic<int64_t> g_launches{0};
+static std::atomic<int> g_knn_variant{0};
+int knn_variant() { return g_knn_variant.load(std::memory_order_relaxed); }
+static std::atomic<int> g_knn_bps{0}, g_knn_wpb{4};
+int knn_blocks_per_sm() { return g_knn_bps.load(std::memory_order_relaxed); }
+int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ---------------------------------------------------------- scratch memory
@@ -76,6 +81,7 @@ ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
                        int sorted, double* dist, int64_t* idx, cudaStream_t s);
 ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
                        cudaStream_t s);
+ckd_status knn_stats(int enable, int64_t* out);
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s);
@@ -107,6 +113,11 @@ static void release_tree(ckd_tree* t) {
   cudaFree(t->cell);
   cudaFree(t->pts);
   cudaFree(t->ids);
+  cudaFree(t->box32);
+  cudaFree(t->pts32);
+  cudaFree(t->pair);
+  cudaFree(t->cell32);
+  cudaFree(t->centre);
   delete t;
 }
 
@@ -272,6 +283,29 @@ ckd_status ckd_knn_ordered(const ckd_tree* t, const double* q, int64_t nq, const
 }
 
 int64_t ckd_launch_count(void) { return g_launches.load(); }
+
+ckd_status ckd_knn_stats(int enable, int64_t* out8) { return knn_stats(enable, out8); }
+
+ckd_status ckd_set_knn_variant(int variant) {
+  if (variant < 0 || variant > 5) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..5");
+  g_knn_variant.store(variant);
+  return CKD_OK;
+}
+
+ckd_status ckd_set_tuning(int key, int value) {
+  switch (key) {
+    case 0: return ckd_set_knn_variant(value);
+    case 1:
+      if (value < 0 || value > 64) return fail(CKD_ERR_BAD_ARG, "blocks per SM must be 0..64");
+      g_knn_bps.store(value);
+      return CKD_OK;
+    case 2:
+      if (value < 1 || value > 8) return fail(CKD_ERR_BAD_ARG, "warps per block must be 1..8");
+      g_knn_wpb.store(value);
+      return CKD_OK;
+  }
+  return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
+}
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                         double* dist, int64_t* idx, void* stream) {

@@ -19,6 +19,7 @@
 // sorted by original index and "first occurrence" (Fortran minloc/maxloc,
 // cosmokdtree.f90:372-373) is the lowest index holding the extreme.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -445,6 +446,88 @@ __global__ void k_leaf_box(const NodeMeta* __restrict__ meta, int32_t n_nodes, i
   }
 }
 
+// FP32 node boxes rounded outwards (lo down, hi up): every FP32 gap computed from
+// them is a lower bound of the FP64 gap up to the screen's rounding slack.
+template <int D>
+__global__ void k_box32(const double* __restrict__ box, int32_t n_nodes, float* __restrict__ box32) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n_nodes * 2 * D) return;
+  double v = box[i];
+  box32[i] = (i & 1) ? __double2float_ru(v) : __double2float_rd(v);
+}
+
+// Each point relative to its leaf's box centre, rounded to FP32, packed in float4s.
+template <int D>
+__global__ void k_pts32(const NodeMeta* __restrict__ meta, int32_t n_nodes, int leaf,
+                        const double* __restrict__ box, const double* __restrict__ Pf, int64_t n,
+                        float4* __restrict__ P32) {
+  constexpr int NV = (D + 3) / 4;
+  int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n_nodes) return;
+  NodeMeta m = meta[a];
+  if (m.left >= 0) return;
+  double c[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+    c[j] = leaf_centre(box[(int64_t)a * 2 * D + 2 * j], box[(int64_t)a * 2 * D + 2 * j + 1]);
+  for (int i = 0; i < m.count; ++i) {
+    int64_t p = (int64_t)m.start + i;
+    float v[4 * NV];
+#pragma unroll
+    for (int j = 0; j < 4 * NV; ++j)
+      v[j] = j < D ? __double2float_rn(__dsub_rn(Pf[(int64_t)j * n + p], c[j < D ? j : 0])) : 0.0f;
+#pragma unroll
+    for (int h = 0; h < NV; ++h)
+      P32[p * NV + h] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+  }
+}
+
+// Bottom-up search records: inward-rounded FP32 cells, FP64 leaf centres, and for
+// each internal node the child-pair record (both children's outward FP32 boxes,
+// ids and leaf flags) so one load serves a whole expansion.
+template <int D>
+__global__ void k_search_records(const NodeMeta* __restrict__ meta, int32_t n_nodes,
+                                 const double* __restrict__ box, const double* __restrict__ cell,
+                                 float4* __restrict__ pair, float* __restrict__ cell32,
+                                 double* __restrict__ centre) {
+  constexpr int NV = (D + 3) / 4;
+  constexpr int PF = 4 * NV + 1;
+  int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n_nodes) return;
+  NodeMeta m = meta[a];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    cell32[(int64_t)a * 2 * D + 2 * j] = __double2float_ru(cell[(int64_t)a * 2 * D + 2 * j]);
+    cell32[(int64_t)a * 2 * D + 2 * j + 1] = __double2float_rd(cell[(int64_t)a * 2 * D + 2 * j + 1]);
+  }
+  if (m.left < 0) {
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      centre[(int64_t)a * D + j] =
+          leaf_centre(box[(int64_t)a * 2 * D + 2 * j], box[(int64_t)a * 2 * D + 2 * j + 1]);
+    return;
+  }
+  float4* rec = pair + (int64_t)a * PF;
+  for (int side = 0; side < 2; ++side) {
+    int32_t c = m.left + side;
+    float lo[4 * NV], hi[4 * NV];
+#pragma unroll
+    for (int j = 0; j < 4 * NV; ++j) {
+      lo[j] = j < D ? __double2float_rd(box[(int64_t)c * 2 * D + 2 * (j < D ? j : 0)]) : 0.0f;
+      hi[j] = j < D ? __double2float_ru(box[(int64_t)c * 2 * D + 2 * (j < D ? j : 0) + 1]) : 0.0f;
+    }
+#pragma unroll
+    for (int h = 0; h < NV; ++h) {
+      rec[side * 2 * NV + h] = make_float4(lo[4 * h], lo[4 * h + 1], lo[4 * h + 2], lo[4 * h + 3]);
+      rec[side * 2 * NV + NV + h] =
+          make_float4(hi[4 * h], hi[4 * h + 1], hi[4 * h + 2], hi[4 * h + 3]);
+    }
+  }
+  int4 info = make_int4(m.left, m.left + 1, meta[m.left].left < 0 ? 1 : 0,
+                        meta[m.left + 1].left < 0 ? 1 : 0);
+  rec[4 * NV] = *reinterpret_cast<float4*>(&info);
+}
+
 template <int D>
 __global__ void k_root_init(NodeMeta* meta, double* cell, unsigned long long* keys, int32_t n,
                             const double* L, int periodic) {
@@ -659,6 +742,29 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(cudaMemcpyAsync(t->meta, B.meta, sizeof(NodeMeta) * n_nodes, cudaMemcpyDeviceToDevice, s));
   CKD_CUDA(cudaMemcpyAsync(t->box, B.box, sizeof(double) * 2 * D * n_nodes, cudaMemcpyDeviceToDevice, s));
   CKD_CUDA(cudaMemcpyAsync(t->cell, B.cell, sizeof(double) * 2 * D * n_nodes, cudaMemcpyDeviceToDevice, s));
+  // FP32 screening copies.  The node-gap slack per axis is 2^-21 * (|q| + B) with
+  // B bounding every stored coordinate (and the box side when periodic); the
+  // screen is disabled for coordinates near the FP32 range.
+  t->screen_ok = true;
+  for (int j = 0; j < D; ++j) {
+    double b = std::max(std::fabs(rlo[j]), std::fabs(rhi[j])) + (t->periodic ? t->L[j] : 0.0);
+    if (!(b < 1e18)) t->screen_ok = false;
+    t->slack[j] = (float)(b * (1.0 + 1e-6));
+  }
+  constexpr int NV = (D + 3) / 4;
+  CKD_CUDA(cudaMalloc((void**)&t->box32, sizeof(float) * 2 * D * n_nodes));
+  CKD_CUDA(cudaMalloc((void**)&t->pts32, sizeof(float4) * NV * n));
+  k_box32<D><<<(unsigned)cdiv((int64_t)n_nodes * 2 * D, 256), 256, 0, s>>>(t->box, n_nodes, t->box32);
+  CKD_LAUNCH_CHECK();
+  k_pts32<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(t->meta, n_nodes, leaf, t->box, t->pts, n,
+                                                          t->pts32);
+  CKD_LAUNCH_CHECK();
+  CKD_CUDA(cudaMalloc((void**)&t->pair, sizeof(float4) * pair_f4(D) * n_nodes));
+  CKD_CUDA(cudaMalloc((void**)&t->cell32, sizeof(float) * 2 * D * n_nodes));
+  CKD_CUDA(cudaMalloc((void**)&t->centre, sizeof(double) * D * n_nodes));
+  k_search_records<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(
+      t->meta, n_nodes, t->box, t->cell, t->pair, t->cell32, t->centre);
+  CKD_LAUNCH_CHECK();
   CKD_CUDA(cudaStreamSynchronize(s));
   if (err) return fail(CKD_ERR_CUDA, "internal error: inconsistent partition in build");
   // leaves = (nodes + 1) / 2 for a full binary tree

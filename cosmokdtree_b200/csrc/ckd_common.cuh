@@ -36,6 +36,12 @@ void note_launch();
     if (_s != CKD_OK) return _s;         \
   } while (0)
 
+// kNN kernel choice: 0 automatic, 1 FP64-only traversal, 2 FP32-screened traversal
+int knn_variant();
+// tuning knobs (see ckd_set_tuning): blocks-per-SM cap (0 = none), warps per block
+int knn_blocks_per_sm();
+int knn_warps_per_block();
+
 // stream-ordered scratch allocation from a per-device pool
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t dev_free(void* p, cudaStream_t s);
@@ -67,7 +73,28 @@ struct TreeView {
   const double* cell;        // [n_nodes][2d] sliding-midpoint cell (reference node bounds)
   const double* pts;         // SoA [d][n], leaf order
   const int32_t* ids;        // [n] original index per leaf-ordered point
+  // FP32 screening copies (see leaf_frame): node boxes rounded outwards, and
+  // each point relative to its leaf's box centre, 1 (d <= 4) or 2 float4 per point
+  const float* box32;        // [n_nodes][2d]
+  const float4* pts32;       // [n][(d + 3) / 4]
+  float slack[CKD_MAX_D];    // per-axis absolute slack of FP32 node-box gaps
+  // bottom-up search records
+  const float4* pair;        // per internal node: both children's FP32 boxes + ids/flags
+  const float* cell32;       // [n_nodes][2d] cells rounded inwards (lo up, hi down)
+  const double* centre;      // [n_nodes][d] leaf centres (leaf_centre of the FP64 box)
 };
+
+// Child-pair record of an internal node, (4 * NV + 1) float4s with NV = (d+3)/4:
+// left lo[NV], left hi[NV], right lo[NV], right hi[NV], then int4 {left node,
+// right node, left is-leaf, right is-leaf}.
+__host__ __device__ constexpr int pair_f4(int d) { return 4 * ((d + 3) / 4) + 1; }
+
+// Leaf frame used by the FP32 screen: centre c = 0.5 * (lo + hi) of the leaf's
+// FP64 box (the same separately rounded operations when the FP32 copy is made
+// and when a query is screened), and the half-extent R >= |p - c| of its points.
+__device__ __forceinline__ double leaf_centre(double lo, double hi) {
+  return __dmul_rn(0.5, __dadd_rn(lo, hi));
+}
 
 // --------------------------------------------------------- exact FP64 math
 // Every FP64 product and sum below is separately rounded (explicit _rn
@@ -144,6 +171,13 @@ struct ckd_tree {
   double* cell = nullptr;
   double* pts = nullptr;
   int32_t* ids = nullptr;
+  float* box32 = nullptr;
+  float4* pts32 = nullptr;
+  float slack[CKD_MAX_D] = {0};
+  bool screen_ok = false;  // FP32 screen usable (coordinates well inside FP32 range)
+  float4* pair = nullptr;
+  float* cell32 = nullptr;
+  double* centre = nullptr;
   ckd::TreeView view() const {
     ckd::TreeView v;
     v.n = (int32_t)n;
@@ -156,6 +190,12 @@ struct ckd_tree {
     v.cell = cell;
     v.pts = pts;
     v.ids = ids;
+    v.box32 = box32;
+    v.pts32 = pts32;
+    for (int j = 0; j < CKD_MAX_D; ++j) v.slack[j] = slack[j];
+    v.pair = pair;
+    v.cell32 = cell32;
+    v.centre = centre;
     return v;
   }
 };

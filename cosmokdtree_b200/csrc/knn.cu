@@ -21,6 +21,16 @@ namespace ckd {
 namespace {
 
 constexpr int kStack = 96;   // per-warp traversal stack in shared memory
+
+// process-wide traversal statistics of the screened kernel (diagnostics)
+__device__ unsigned long long g_knn_stats[8];
+bool g_stats_on = false;
+unsigned long long* knn_stats_buffer() {
+  if (!g_stats_on) return nullptr;
+  void* p = nullptr;
+  cudaGetSymbolAddress(&p, g_knn_stats);
+  return reinterpret_cast<unsigned long long*>(p);
+}
 constexpr int kSmemK = 64;   // largest k kept in shared memory
 
 // ---------------------------------------------------------- heap storage
@@ -242,10 +252,1140 @@ __global__ void __launch_bounds__(128) k_knn_rows(TreeView tv, const double* __r
   }
 }
 
+// ====================================================== FP32-screened search
+// Same traversal and result as k_knn_smem, with two changes that cut the
+// instruction count per query:
+//  * leaves are screened in FP32 on leaf-relative coordinates: a point's FP32
+//    lower bound of its FP64 squared distance is compared with the current k-th
+//    (rounded up); only points that can still enter are evaluated in FP64 with
+//    the reference arithmetic and ranked exactly by (d2, id);
+//  * inserts are deferred per 32-point chunk (candidate bitmask first), and the
+//    heap keys are the FP64 bit patterns compared as uint64, siblings adjacent
+//    (1-based heap) so one 16-byte shared load reads both children.
+// Node pruning uses the outward-rounded FP32 boxes minus a rounding slack.
+
+constexpr float kTwoM21 = 4.76837158203125e-07f;  // 2^-21
+constexpr float kShrink = 0.99999905f;             // 1 - 2^-20
+
+// heap stride per lane (in slots): >= k + 1 and == 2 mod 16, so the 8 lanes of a
+// 16-byte shared-memory phase hit distinct banks for the same slot
+__host__ __device__ inline int heap_stride(int k) {
+  int s = k + 1;
+  return s + ((2 - s) % 16 + 16) % 16;
+}
+
+template <int D, bool PER>
+struct QueryScreen {
+  float q32[D];
+  float dlt[D];  // node-gap slack 2^-21 (|q| + B)
+};
+
+template <int D, bool PER>
+__device__ __forceinline__ float node_mind_lb(const TreeView& tv, const QueryScreen<D, PER>& qs,
+                                              int32_t node) {
+  const float* b = tv.box32 + (int64_t)node * 2 * D;
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float2 lh = __ldg(reinterpret_cast<const float2*>(b) + j);
+    float x = qs.q32[j], g;
+    if (x >= lh.x - qs.dlt[j] && x <= lh.y + qs.dlt[j]) {
+      g = 0.0f;
+    } else if (!PER) {
+      g = fmaxf(lh.x - x, x - lh.y) - qs.dlt[j];
+    } else {
+      float L = (float)tv.L[j];
+      float t1 = fabsf(x - lh.x), t2 = fabsf(x - lh.y);
+      g = fminf(fminf(t1, L - t1), fminf(t2, L - t2)) - qs.dlt[j];
+    }
+    g = fmaxf(g, 0.0f);
+    s = fmaf(g, g, s);
+  }
+  return s * kShrink;
+}
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_knn_screen(TreeView tv, const double* __restrict__ Q,
+                                                    const int32_t* __restrict__ order, int64_t nq,
+                                                    int k, int sorted, int32_t* __restrict__ gstack,
+                                                    int stack_len, double* __restrict__ dist,
+                                                    int64_t* __restrict__ idx,
+                                                    unsigned long long* __restrict__ stats) {
+  constexpr int NV = (D + 3) / 4;
+  // traversal statistics (only when `stats` is given): pops, needed pops, leaf
+  // visits, points screened, warp phase-2 rounds, FP64 evaluations, inserts,
+  // lanes active on leaf visits
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int KS = heap_stride(k);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem) + (size_t)w * 32 * KS;
+  int32_t* ids = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned long long*>(smem) +
+                                            (size_t)nw * 32 * KS) +
+                 (size_t)w * 32 * KS;
+  int64_t gw = (int64_t)blockIdx.x * nw + w;
+  int32_t* stk = gstack ? gstack + gw * stack_len
+                        : reinterpret_cast<int32_t*>(reinterpret_cast<int32_t*>(
+                              reinterpret_cast<unsigned long long*>(smem) + (size_t)nw * 32 * KS) +
+                                                     (size_t)nw * 32 * KS) +
+                              (size_t)w * kStack;
+  int64_t slot = gw * 32 + lane;
+  const bool valid = slot < nq;
+  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    q[j] = valid ? Q[qi * D + j] : 0.0;
+    qs.q32[j] = __double2float_rn(q[j]);
+    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+  }
+  unsigned long long* hk = keys + lane * KS;  // 1-based: slots 1..k
+  int32_t* hi = ids + lane * KS;
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  for (int s = 1; s <= k; ++s) {
+    hk[s] = kHugeKey;
+    hi[s] = -1;
+  }
+  unsigned long long wkey = kHugeKey;
+  int32_t wid = -1;
+  float wd32 = valid ? FLT_MAX : -1.0f;
+
+  int top = 0;
+  if (lane == 0) stk[0] = 0;
+  __syncwarp();
+  while (top >= 0) {
+    int32_t node = stk[top];
+    --top;
+    __syncwarp();
+    NodeMeta m = load_meta(tv.meta, node);
+    bool need = node_mind_lb<D, PER>(tv, qs, node) <= wd32;
+    unsigned nm = __ballot_sync(0xffffffffu, need);
+    if (stats) st[0] += 1;
+    if (nm == 0) continue;
+    if (stats) st[1] += 1;
+    if (m.left >= 0) {
+      float qa = 0.0f;
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        if (j == m.axis) qa = qs.q32[j];
+      unsigned lv = __ballot_sync(0xffffffffu, need && (double)qa < m.split);
+      bool left_first = 2 * __popc(lv) >= __popc(nm);
+      if (lane == 0) {
+        stk[top + 1] = left_first ? m.left + 1 : m.left;
+        stk[top + 2] = left_first ? m.left : m.left + 1;
+      }
+      top += 2;
+      __syncwarp();
+      continue;
+    }
+    // ---- leaf: frame (query relative to the leaf centre) and error bounds
+    if (stats) {
+      st[2] += 1;
+      st[3] += m.count;
+      st[7] += __popc(nm);
+    }
+    float qr[D], e[D];
+    {
+      const double* b = tv.box + (int64_t)node * 2 * D;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        double lo = __ldg(&b[2 * j]), hh = __ldg(&b[2 * j + 1]);
+        double c = leaf_centre(lo, hh);
+        double r = fmax(c - lo, hh - c);
+        double x = q[j] - c;
+        if (PER) {
+          double h = 0.5 * tv.L[j];
+          if (x > h) x -= tv.L[j];
+          else if (x < -h) x += tv.L[j];
+        }
+        qr[j] = __double2float_rn(x);
+        e[j] = kTwoM21 * (float)(r + fabs(x) + (PER ? tv.L[j] : 0.0)) * 1.0001f + 1e-37f;
+      }
+    }
+    for (int base = 0; base < m.count; base += 32) {
+      const int cnt = min(32, m.count - base);
+      const int32_t p0 = m.start + base;
+      unsigned mask = 0;
+      for (int i = 0; i < cnt; ++i) {
+        float v[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+          v[4 * h] = f.x;
+          v[4 * h + 1] = f.y;
+          v[4 * h + 2] = f.z;
+          v[4 * h + 3] = f.w;
+        }
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float a = fabsf(v[j] - qr[j]);
+          if (PER) a = fminf(a, (float)tv.L[j] - a);
+          a = fmaxf(a - e[j], 0.0f);
+          s = fmaf(a, a, s);
+        }
+        if (s * kShrink <= wd32) mask |= 1u << i;
+      }
+      if (!need) mask = 0;
+      if (stats) {
+        st[4] += __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
+        st[5] += __popc(mask);
+      }
+      while (mask) {
+        int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        int32_t p = p0 + i;
+        double d2 = point_d2<D, PER>(tv, q, p);
+        unsigned long long key = (unsigned long long)__double_as_longlong(d2);
+        if (key > wkey) continue;
+        int32_t id = __ldg(&tv.ids[p]);
+        if (key == wkey && id >= wid) continue;
+        // replace the root (slot 1) and sift down
+        if (stats) st[6] += 1;
+        int s = 1;
+        for (;;) {
+          int l = 2 * s;
+          if (l > k) break;
+          unsigned long long kc;
+          int32_t ic;
+          int c;
+          if (l < k) {
+            ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(hk + l);
+            int2 ii = *reinterpret_cast<const int2*>(hi + l);
+            bool right = kk.x < kk.y || (kk.x == kk.y && ii.x < ii.y);
+            kc = right ? kk.y : kk.x;
+            ic = right ? ii.y : ii.x;
+            c = right ? l + 1 : l;
+          } else {
+            kc = hk[l];
+            ic = hi[l];
+            c = l;
+          }
+          if (!(key < kc || (key == kc && id < ic))) break;
+          hk[s] = kc;
+          hi[s] = ic;
+          s = c;
+        }
+        hk[s] = key;
+        hi[s] = id;
+        wkey = hk[1];
+        wid = hi[1];
+        wd32 = __double2float_ru(__longlong_as_double((long long)wkey));
+      }
+    }
+  }
+  if (stats) {
+    // pops, needed, leaves, points and rounds are warp-uniform: count them once
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = st[c];
+      if (c == 5 || c == 6) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      }
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+  // ---- ascending (d2, id) by heap sort, then a coalesced write-out
+  if (sorted) {
+    for (int end = k; end > 1; --end) {
+      unsigned long long key = hk[end];
+      int32_t id = hi[end];
+      hk[end] = hk[1];
+      hi[end] = hi[1];
+      int s = 1;
+      for (;;) {
+        int l = 2 * s;
+        if (l >= end) break;
+        int c = l;
+        unsigned long long kc = hk[l];
+        int32_t ic = hi[l];
+        if (l + 1 < end) {
+          unsigned long long kr = hk[l + 1];
+          int32_t ir = hi[l + 1];
+          if (kc < kr || (kc == kr && ic < ir)) {
+            c = l + 1;
+            kc = kr;
+            ic = ir;
+          }
+        }
+        if (!(key < kc || (key == kc && id < ic))) break;
+        hk[s] = kc;
+        hi[s] = ic;
+        s = c;
+      }
+      hk[s] = key;
+      hi[s] = id;
+    }
+  }
+  __syncwarp();
+  for (int qq = 0; qq < 32; ++qq) {
+    int64_t s2 = gw * 32 + qq;
+    if (s2 >= nq) break;
+    int64_t row = order ? (int64_t)order[s2] : s2;
+    const unsigned long long* rk = keys + qq * KS + 1;
+    const int32_t* ri = ids + qq * KS + 1;
+    for (int j = lane; j < k; j += 32) {
+      int32_t id = ri[j];
+      dist[row * k + j] = sqrt(__longlong_as_double((long long)rk[j]));
+      idx[row * k + j] = id < 0 ? -2 : (int64_t)id;
+    }
+  }
+}
+
+// ================================================= per-lane traversal variant
+// Each lane walks the tree for its own query: both children's FP32 boxes are
+// tested when a node is expanded, the nearer child is taken and the other pushed
+// with its bound on a per-lane stack (registers / local memory), so entries that
+// the shrinking k-th distance has pruned are dropped without reloading a node.
+// Lanes descend until they reach a leaf, then scan leaves together
+// (while-while structure), with the same FP32 screen, FP64 recheck and heap as
+// k_knn_screen.
+constexpr int kLaneStack = 64;
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __restrict__ Q,
+                                                  const int32_t* __restrict__ order, int64_t nq,
+                                                  int k, int sorted, double* __restrict__ dist,
+                                                  int64_t* __restrict__ idx,
+                                                  unsigned long long* __restrict__ stats) {
+  constexpr int NV = (D + 3) / 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int KS = heap_stride(k);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem) + (size_t)w * 32 * KS;
+  int32_t* ids = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned long long*>(smem) +
+                                            (size_t)nw * 32 * KS) +
+                 (size_t)w * 32 * KS;
+  int64_t gw = (int64_t)blockIdx.x * nw + w;
+  int64_t slot = gw * 32 + lane;
+  const bool valid = slot < nq;
+  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    q[j] = valid ? Q[qi * D + j] : 0.0;
+    qs.q32[j] = __double2float_rn(q[j]);
+    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+  }
+  unsigned long long* hk = keys + lane * KS;
+  int32_t* hi = ids + lane * KS;
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  for (int s = 1; s <= k; ++s) {
+    hk[s] = kHugeKey;
+    hi[s] = -1;
+  }
+  unsigned long long wkey = kHugeKey;
+  int32_t wid = -1;
+  float wd32 = FLT_MAX;
+
+  int32_t sn[kLaneStack];
+  float sd[kLaneStack];
+  int top = 0;
+  int32_t node = valid ? 0 : -1;
+  while (node >= 0) {
+    // ---- descend to a leaf, nearer child first
+    NodeMeta m = load_meta(tv.meta, node);
+    while (node >= 0 && m.left >= 0) {
+      if (stats) st[0] += 1;
+      float ml = node_mind_lb<D, PER>(tv, qs, m.left);
+      float mr = node_mind_lb<D, PER>(tv, qs, m.left + 1);
+      bool nl = ml <= wd32, nr = mr <= wd32;
+      if (nl && nr) {
+        bool lf = ml <= mr;
+        sn[top] = lf ? m.left + 1 : m.left;
+        sd[top] = lf ? mr : ml;
+        ++top;
+        node = lf ? m.left : m.left + 1;
+      } else if (nl || nr) {
+        node = nl ? m.left : m.left + 1;
+      } else {
+        node = -1;
+        while (top > 0) {
+          --top;
+          if (sd[top] <= wd32) {
+            node = sn[top];
+            break;
+          }
+        }
+      }
+      if (node >= 0) m = load_meta(tv.meta, node);
+    }
+    if (node < 0) break;
+    // ---- scan the leaf
+    if (stats) {
+      st[2] += 1;
+      st[3] += m.count;
+    }
+    float qr[D], e[D];
+    {
+      const double* b = tv.box + (int64_t)node * 2 * D;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        double lo = __ldg(&b[2 * j]), hh = __ldg(&b[2 * j + 1]);
+        double c = leaf_centre(lo, hh);
+        double r = fmax(c - lo, hh - c);
+        double x = q[j] - c;
+        if (PER) {
+          double h = 0.5 * tv.L[j];
+          if (x > h) x -= tv.L[j];
+          else if (x < -h) x += tv.L[j];
+        }
+        qr[j] = __double2float_rn(x);
+        e[j] = kTwoM21 * (float)(r + fabs(x) + (PER ? tv.L[j] : 0.0)) * 1.0001f + 1e-37f;
+      }
+    }
+    for (int base = 0; base < m.count; base += 32) {
+      const int cnt = min(32, m.count - base);
+      const int32_t p0 = m.start + base;
+      unsigned mask = 0;
+      for (int i = 0; i < cnt; ++i) {
+        float v[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+          v[4 * h] = f.x;
+          v[4 * h + 1] = f.y;
+          v[4 * h + 2] = f.z;
+          v[4 * h + 3] = f.w;
+        }
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float a = fabsf(v[j] - qr[j]);
+          if (PER) a = fminf(a, (float)tv.L[j] - a);
+          a = fmaxf(a - e[j], 0.0f);
+          s = fmaf(a, a, s);
+        }
+        if (s * kShrink <= wd32) mask |= 1u << i;
+      }
+      if (stats) st[5] += __popc(mask);
+      while (mask) {
+        int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        int32_t p = p0 + i;
+        double d2 = point_d2<D, PER>(tv, q, p);
+        unsigned long long key = (unsigned long long)__double_as_longlong(d2);
+        if (key > wkey) continue;
+        int32_t id = __ldg(&tv.ids[p]);
+        if (key == wkey && id >= wid) continue;
+        if (stats) st[6] += 1;
+        int s = 1;
+        for (;;) {
+          int l = 2 * s;
+          if (l > k) break;
+          unsigned long long kc;
+          int32_t ic;
+          int c;
+          if (l < k) {
+            ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(hk + l);
+            int2 ii = *reinterpret_cast<const int2*>(hi + l);
+            bool right = kk.x < kk.y || (kk.x == kk.y && ii.x < ii.y);
+            kc = right ? kk.y : kk.x;
+            ic = right ? ii.y : ii.x;
+            c = right ? l + 1 : l;
+          } else {
+            kc = hk[l];
+            ic = hi[l];
+            c = l;
+          }
+          if (!(key < kc || (key == kc && id < ic))) break;
+          hk[s] = kc;
+          hi[s] = ic;
+          s = c;
+        }
+        hk[s] = key;
+        hi[s] = id;
+        wkey = hk[1];
+        wid = hi[1];
+        wd32 = __double2float_ru(__longlong_as_double((long long)wkey));
+      }
+    }
+    // ---- next: pop the nearest pending subtree still within reach
+    node = -1;
+    while (top > 0) {
+      --top;
+      if (sd[top] <= wd32) {
+        node = sn[top];
+        break;
+      }
+    }
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = st[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+  if (sorted && valid) {
+    for (int end = k; end > 1; --end) {
+      unsigned long long key = hk[end];
+      int32_t id = hi[end];
+      hk[end] = hk[1];
+      hi[end] = hi[1];
+      int s = 1;
+      for (;;) {
+        int l = 2 * s;
+        if (l >= end) break;
+        int c = l;
+        unsigned long long kc = hk[l];
+        int32_t ic = hi[l];
+        if (l + 1 < end) {
+          unsigned long long kr = hk[l + 1];
+          int32_t ir = hi[l + 1];
+          if (kc < kr || (kc == kr && ic < ir)) {
+            c = l + 1;
+            kc = kr;
+            ic = ir;
+          }
+        }
+        if (!(key < kc || (key == kc && id < ic))) break;
+        hk[s] = kc;
+        hi[s] = ic;
+        s = c;
+      }
+      hk[s] = key;
+      hi[s] = id;
+    }
+  }
+  __syncwarp();
+  for (int qq = 0; qq < 32; ++qq) {
+    int64_t s2 = gw * 32 + qq;
+    if (s2 >= nq) break;
+    int64_t row = order ? (int64_t)order[s2] : s2;
+    const unsigned long long* rk = keys + qq * KS + 1;
+    const int32_t* ri = ids + qq * KS + 1;
+    for (int j = lane; j < k; j += 32) {
+      int32_t id = ri[j];
+      dist[row * k + j] = sqrt(__longlong_as_double((long long)rk[j]));
+      idx[row * k + j] = id < 0 ? -2 : (int64_t)id;
+    }
+  }
+}
+
+// ===================================================== bottom-up search (v4)
+// Per-lane search that starts at the query's own leaf and climbs: after a
+// subtree C is exhausted, the search stops if the ball of the current k-th
+// distance lies inside C's sliding-midpoint cell (cells partition the box, so no
+// point outside C can be closer; under periodic wrap the ball then lies inside
+// the fundamental box, so no image can be closer either); otherwise C's sibling
+// subtree is explored top-down, nearer child first, pruned by FP32 boxes, and C
+// moves to its parent.  Leaves are screened in FP32 and ranked exactly in FP64
+// as in k_knn_screen.
+
+struct LaneHeap {
+  unsigned long long* hk;  // 1-based slots 1..k (FP64 bit patterns)
+  int32_t* hi;
+  int k;
+  int n;  // real entries so far; below k the slots are an unordered list
+  unsigned long long wkey;
+  int32_t wid;
+  float wd32;  // current k-th squared distance rounded up to FP32
+};
+
+// sift (key, id) down from slot s within slots 1..end
+__device__ __forceinline__ void lane_sift(LaneHeap& H, int s, int end, unsigned long long key,
+                                          int32_t id) {
+  for (;;) {
+    int l = 2 * s;
+    if (l > end) break;
+    unsigned long long kc;
+    int32_t ic;
+    int c;
+    if (l < end) {
+      ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(H.hk + l);
+      int2 ii = *reinterpret_cast<const int2*>(H.hi + l);
+      bool right = kk.x < kk.y || (kk.x == kk.y && ii.x < ii.y);
+      kc = right ? kk.y : kk.x;
+      ic = right ? ii.y : ii.x;
+      c = right ? l + 1 : l;
+    } else {
+      kc = H.hk[l];
+      ic = H.hi[l];
+      c = l;
+    }
+    if (!(key < kc || (key == kc && id < ic))) break;
+    H.hk[s] = kc;
+    H.hi[s] = ic;
+    s = c;
+  }
+  H.hk[s] = key;
+  H.hi[s] = id;
+}
+
+__device__ __forceinline__ void lane_heapify(LaneHeap& H, int end) {
+  for (int s = end / 2; s >= 1; --s) lane_sift(H, s, end, H.hk[s], H.hi[s]);
+}
+
+// A candidate that ranks before the current k-th.  While fewer than k entries
+// are held it is appended (the k-th is still the HUGE(0.0) sentinel); the k-th
+// append heapifies once, later candidates replace the root and sift down.
+__device__ __forceinline__ void lane_heap_insert(LaneHeap& H, unsigned long long key, int32_t id) {
+  if (H.n < H.k) {
+    ++H.n;
+    H.hk[H.n] = key;
+    H.hi[H.n] = id;
+    if (H.n < H.k) return;
+    lane_heapify(H, H.k);
+  } else {
+    lane_sift(H, 1, H.k, key, id);
+  }
+  H.wkey = H.hk[1];
+  H.wid = H.hi[1];
+  H.wd32 = __double2float_ru(__longlong_as_double((long long)H.wkey));
+}
+
+// pad with (HUGE(0.0), -1) sentinels when fewer than k points were found
+__device__ __forceinline__ void lane_heap_finish(LaneHeap& H) {
+  if (H.n == H.k) return;
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  for (int s = H.n + 1; s <= H.k; ++s) {
+    H.hk[s] = kHugeKey;
+    H.hi[s] = -1;
+  }
+  H.n = H.k;
+  lane_heapify(H, H.k);
+}
+
+__device__ __forceinline__ void lane_heap_sort(LaneHeap& H) {
+  for (int end = H.k; end > 1; --end) {
+    unsigned long long key = H.hk[end];
+    int32_t id = H.hi[end];
+    H.hk[end] = H.hk[1];
+    H.hi[end] = H.hi[1];
+    lane_sift(H, 1, end - 1, key, id);
+  }
+}
+
+// FP32 lower bound of a child box gap from a child-pair record side
+template <int D, bool PER>
+__device__ __forceinline__ float rec_mind_lb(const TreeView& tv, const QueryScreen<D, PER>& qs,
+                                             const float (&lo)[4 * ((D + 3) / 4)],
+                                             const float (&hi)[4 * ((D + 3) / 4)]) {
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float x = qs.q32[j], g;
+    if (x >= lo[j] - qs.dlt[j] && x <= hi[j] + qs.dlt[j]) {
+      g = 0.0f;
+    } else if (!PER) {
+      g = fmaxf(lo[j] - x, x - hi[j]) - qs.dlt[j];
+    } else {
+      float L = (float)tv.L[j];
+      float t1 = fabsf(x - lo[j]), t2 = fabsf(x - hi[j]);
+      g = fminf(fminf(t1, L - t1), fminf(t2, L - t2)) - qs.dlt[j];
+    }
+    g = fmaxf(g, 0.0f);
+    s = fmaf(g, g, s);
+  }
+  return s * kShrink;
+}
+
+// Screen one leaf and insert the points that can enter (see k_knn_screen).
+template <int D, bool PER>
+__device__ __forceinline__ void lane_scan_leaf(const TreeView& tv, const double (&q)[D],
+                                               int32_t node, int32_t start, int32_t count,
+                                               LaneHeap& H, unsigned long long* st) {
+  constexpr int NV = (D + 3) / 4;
+  float qr[D], e[D];
+  const float* b32 = tv.box32 + (int64_t)node * 2 * D;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double c = __ldg(&tv.centre[(int64_t)node * D + j]);
+    float2 lh = __ldg(reinterpret_cast<const float2*>(b32) + j);
+    double r = fmax(c - (double)lh.x, (double)lh.y - c);  // >= |p - c| for every point
+    double x = q[j] - c;
+    double wrap = 0.0;
+    if (PER) {
+      double h = 0.5 * tv.L[j];
+      if (x > h) x -= tv.L[j];
+      else if (x < -h) x += tv.L[j];
+      if (r + fabs(x) > 0.45 * tv.L[j]) wrap = tv.L[j];  // minimum image may wrap
+    }
+    qr[j] = __double2float_rn(x);
+    e[j] = kTwoM21 * (float)(r + fabs(x) + wrap) * 1.0001f + 1e-37f;
+  }
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  for (int base = 0; base < count; base += 32) {
+    const int cnt = min(32, count - base);
+    const int32_t p0 = start + base;
+    unsigned mask = 0;
+    for (int i = 0; i < cnt; ++i) {
+      float v[4 * NV];
+#pragma unroll
+      for (int h = 0; h < NV; ++h) {
+        float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+        v[4 * h] = f.x;
+        v[4 * h + 1] = f.y;
+        v[4 * h + 2] = f.z;
+        v[4 * h + 3] = f.w;
+      }
+      float s = 0.0f;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        float a = fabsf(v[j] - qr[j]);
+        if (PER) a = fminf(a, (float)tv.L[j] - a);
+        a = fmaxf(a - e[j], 0.0f);
+        s = fmaf(a, a, s);
+      }
+      if (s * kShrink <= H.wd32) mask |= 1u << i;
+    }
+    if (st) {
+      st[3] += cnt;
+      st[5] += __popc(mask);
+    }
+    while (mask) {
+      int i = __ffs(mask) - 1;
+      mask &= mask - 1;
+      int32_t p = p0 + i;
+      double d2 = point_d2<D, PER>(tv, q, p);
+      unsigned long long key = (unsigned long long)__double_as_longlong(d2);
+      int32_t id;
+      if (H.n < H.k) {
+        if (key >= kHugeKey) continue;  // the strict test against HUGE(0.0)
+        id = __ldg(&tv.ids[p]);
+      } else {
+        if (key > H.wkey) continue;
+        id = __ldg(&tv.ids[p]);
+        if (key == H.wkey && id >= H.wid) continue;
+      }
+      if (st) st[6] += 1;
+      lane_heap_insert(H, key, id);
+    }
+  }
+}
+
+constexpr int kUpStack = 96;
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(256) k_knn_up(TreeView tv, const double* __restrict__ Q,
+                                                const int32_t* __restrict__ order,
+                                                const int32_t* __restrict__ qleaf, int64_t nq,
+                                                int k, int sorted, double* __restrict__ dist,
+                                                int64_t* __restrict__ idx,
+                                                unsigned long long* __restrict__ stats) {
+  constexpr int NV = (D + 3) / 4;
+  constexpr int PF = 4 * NV + 1;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long stv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long* st = stats ? stv : nullptr;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int KS = heap_stride(k);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem) + (size_t)w * 32 * KS;
+  int32_t* ids = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned long long*>(smem) +
+                                            (size_t)nw * 32 * KS) +
+                 (size_t)w * 32 * KS;
+  int64_t gw = (int64_t)blockIdx.x * nw + w;
+  int64_t slot = gw * 32 + lane;
+  const bool valid = slot < nq;
+  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    q[j] = valid ? Q[qi * D + j] : 0.0;
+    qs.q32[j] = __double2float_rn(q[j]);
+    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+  }
+  LaneHeap H;
+  H.hk = keys + lane * KS;
+  H.hi = ids + lane * KS;
+  H.k = k;
+  H.n = 0;
+  H.wkey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  H.wid = -1;
+  H.wd32 = FLT_MAX;
+
+  // ---- per-lane state: climb position, explore stack, pending leaf
+  int32_t pending = -1, C = -1, parent = -1;
+  bool done = !valid;
+  if (valid) {
+    int32_t leaf;
+    NodeMeta lm;
+    if (qleaf) {
+      leaf = qleaf[qi];
+      lm = load_meta(tv.meta, leaf);
+    } else {
+      leaf = 0;
+      lm = load_meta(tv.meta, 0);
+      while (lm.left >= 0) {
+        double qa = 0.0;
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          if (j == lm.axis) qa = q[j];
+        leaf = qa < lm.split ? lm.left : lm.left + 1;
+        lm = load_meta(tv.meta, leaf);
+      }
+    }
+    pending = leaf;
+    C = leaf;
+    parent = lm.parent;
+  }
+  int32_t sn[kUpStack];
+  float sd[kUpStack];
+  int top = 0;
+  for (;;) {
+    // advance this lane until it holds a leaf to scan or has finished
+    while (!done && pending < 0) {
+      if (top > 0) {
+        --top;
+        if (sd[top] > H.wd32) continue;
+        int32_t x = sn[top];
+        if (x < 0) {
+          pending = x & 0x7fffffff;
+          continue;
+        }
+        if (st) st[0] += 1;
+        const float4* r2 = tv.pair + (int64_t)x * PF;
+        float llo[4 * NV], lhi[4 * NV], rlo[4 * NV], rhi[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 a = __ldg(&r2[h]), b = __ldg(&r2[NV + h]);
+          float4 c = __ldg(&r2[2 * NV + h]), d = __ldg(&r2[3 * NV + h]);
+          llo[4 * h] = a.x; llo[4 * h + 1] = a.y; llo[4 * h + 2] = a.z; llo[4 * h + 3] = a.w;
+          lhi[4 * h] = b.x; lhi[4 * h + 1] = b.y; lhi[4 * h + 2] = b.z; lhi[4 * h + 3] = b.w;
+          rlo[4 * h] = c.x; rlo[4 * h + 1] = c.y; rlo[4 * h + 2] = c.z; rlo[4 * h + 3] = c.w;
+          rhi[4 * h] = d.x; rhi[4 * h + 1] = d.y; rhi[4 * h + 2] = d.z; rhi[4 * h + 3] = d.w;
+        }
+        int4 xi = __ldg(reinterpret_cast<const int4*>(&r2[4 * NV]));
+        float ml = rec_mind_lb<D, PER>(tv, qs, llo, lhi);
+        float mr = rec_mind_lb<D, PER>(tv, qs, rlo, rhi);
+        int32_t L = xi.x | (xi.z ? (int32_t)0x80000000 : 0);
+        int32_t R = xi.y | (xi.w ? (int32_t)0x80000000 : 0);
+        bool nl = ml <= H.wd32, nr = mr <= H.wd32;
+        if (nl && nr) {  // the farther first, so the nearer is taken next
+          bool lf = ml <= mr;
+          sn[top] = lf ? R : L;
+          sd[top] = lf ? mr : ml;
+          sn[top + 1] = lf ? L : R;
+          sd[top + 1] = lf ? ml : mr;
+          top += 2;
+        } else if (nl || nr) {
+          sn[top] = nl ? L : R;
+          sd[top] = nl ? ml : mr;
+          top += 1;
+        }
+      } else {
+        if (parent < 0) {
+          done = true;
+          continue;
+        }
+        // stop once the k-th-distance ball lies inside C's cell
+        float r = sqrtf(H.wd32) * 1.0000003f;
+        const float* c32 = tv.cell32 + (int64_t)C * 2 * D;
+        bool inside = true;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float2 cl = __ldg(reinterpret_cast<const float2*>(c32) + j);
+          inside = inside && (qs.q32[j] - r - qs.dlt[j] >= cl.x) &&
+                   (qs.q32[j] + r + qs.dlt[j] <= cl.y);
+        }
+        if (inside) {
+          if (st) st[7] += 1;
+          done = true;
+          continue;
+        }
+        if (st) st[1] += 1;
+        // queue the sibling of C, then climb
+        const float4* rec = tv.pair + (int64_t)parent * PF;
+        int4 info = __ldg(reinterpret_cast<const int4*>(&rec[4 * NV]));
+        const int side = (info.x == C) ? 1 : 0;
+        float lo[4 * NV], hi[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 a = __ldg(&rec[side * 2 * NV + h]), b = __ldg(&rec[side * 2 * NV + NV + h]);
+          lo[4 * h] = a.x; lo[4 * h + 1] = a.y; lo[4 * h + 2] = a.z; lo[4 * h + 3] = a.w;
+          hi[4 * h] = b.x; hi[4 * h + 1] = b.y; hi[4 * h + 2] = b.z; hi[4 * h + 3] = b.w;
+        }
+        float ms = rec_mind_lb<D, PER>(tv, qs, lo, hi);
+        if (ms <= H.wd32) {
+          int32_t S = side ? info.y : info.x;
+          int sleaf = side ? info.w : info.z;
+          sn[0] = S | (sleaf ? (int32_t)0x80000000 : 0);
+          sd[0] = ms;
+          top = 1;
+        }
+        C = parent;
+        parent = load_meta(tv.meta, C).parent;
+      }
+    }
+    if (__all_sync(0xffffffffu, pending < 0)) break;
+    if (pending >= 0) {  // the lanes holding a leaf scan together
+      NodeMeta xm = load_meta(tv.meta, pending);
+      if (st) st[2] += 1;
+      lane_scan_leaf<D, PER>(tv, q, pending, xm.start, xm.count, H, st);
+      pending = -1;
+    }
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = stv[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+  if (valid) {
+    lane_heap_finish(H);
+    if (sorted) lane_heap_sort(H);
+  }
+  __syncwarp();
+  for (int qq = 0; qq < 32; ++qq) {
+    int64_t s2 = gw * 32 + qq;
+    if (s2 >= nq) break;
+    int64_t row = order ? (int64_t)order[s2] : s2;
+    const unsigned long long* rk = keys + qq * KS + 1;
+    const int32_t* ri = ids + qq * KS + 1;
+    for (int j = lane; j < k; j += 32) {
+      int32_t id = ri[j];
+      dist[row * k + j] = sqrt(__longlong_as_double((long long)rk[j]));
+      idx[row * k + j] = id < 0 ? -2 : (int64_t)id;
+    }
+  }
+}
+
+// ============================================ persistent bottom-up search (v5)
+// The bottom-up search of k_knn_up run by a persistent grid: each lane keeps
+// taking queries until the queue is empty.  Per-query work is very uneven
+// (clustered catalogues), so a warp that owned a fixed 32 queries spent most of
+// its instructions on its slowest lane; here a lane that finishes writes its row
+// and takes the next query (queries are handed out in leaf order, 64 at a time
+// per warp from a global counter), so lanes stay busy until the queue drains.
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_knn_persist(TreeView tv, const double* __restrict__ Q,
+                                                     const int32_t* __restrict__ order,
+                                                     const int32_t* __restrict__ qleaf,
+                                                     int64_t nq, int k, int sorted,
+                                                     unsigned long long* __restrict__ counter,
+                                                     double* __restrict__ dist,
+                                                     int64_t* __restrict__ idx,
+                                                     unsigned long long* __restrict__ stats) {
+  constexpr int NV = (D + 3) / 4;
+  constexpr int PF = 4 * NV + 1;
+  constexpr unsigned kBatch = 64;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long stv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long* st = stats ? stv : nullptr;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int KS = heap_stride(k);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem) + (size_t)w * 32 * KS;
+  int32_t* ids = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned long long*>(smem) +
+                                            (size_t)nw * 32 * KS) +
+                 (size_t)w * 32 * KS;
+  LaneHeap H;
+  H.hk = keys + lane * KS;
+  H.hi = ids + lane * KS;
+  H.k = k;
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+
+  // warp-uniform batch of query slots [bnext, bend)
+  unsigned long long bnext = 0, bend = 0;
+  bool exhausted = false;
+  // per-lane state
+  bool active = false;
+  int64_t row = 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+  int32_t pending = -1, C = -1, parent = -1;
+  bool done = true;
+  int32_t sn[kUpStack];
+  float sd[kUpStack];
+  int top = 0;
+  for (;;) {
+    // ---- refill idle lanes
+    unsigned want = __ballot_sync(0xffffffffu, !active);
+    while (want && !exhausted) {
+      if (bnext >= bend) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(counter, (unsigned long long)kBatch);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (b >= (unsigned long long)nq) {
+          exhausted = true;
+          break;
+        }
+        bnext = b;
+        bend = min(b + kBatch, (unsigned long long)nq);
+      }
+      unsigned avail = (unsigned)(bend - bnext);
+      unsigned rank = __popc(want & ((1u << lane) - 1));
+      bool take = !active && rank < avail;
+      unsigned taken = min((unsigned)__popc(want), avail);
+      if (take) {
+        int64_t slot = (int64_t)(bnext + rank);
+        int64_t qi = order ? (int64_t)order[slot] : slot;
+        row = qi;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          q[j] = Q[qi * D + j];
+          qs.q32[j] = __double2float_rn(q[j]);
+          qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+        }
+        H.n = 0;
+        H.wkey = kHugeKey;
+        H.wid = -1;
+        H.wd32 = FLT_MAX;
+        int32_t leaf;
+        NodeMeta lm;
+        if (qleaf) {
+          leaf = qleaf[qi];
+          lm = load_meta(tv.meta, leaf);
+        } else {
+          leaf = 0;
+          lm = load_meta(tv.meta, 0);
+          while (lm.left >= 0) {
+            double qa = 0.0;
+#pragma unroll
+            for (int j = 0; j < D; ++j)
+              if (j == lm.axis) qa = q[j];
+            leaf = qa < lm.split ? lm.left : lm.left + 1;
+            lm = load_meta(tv.meta, leaf);
+          }
+        }
+        pending = leaf;
+        C = leaf;
+        parent = lm.parent;
+        top = 0;
+        done = false;
+        active = true;
+      }
+      bnext += taken;
+      want = __ballot_sync(0xffffffffu, !active);
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+
+    // ---- advance each active lane to a leaf or to completion
+    while (active && !done && pending < 0) {
+      if (top > 0) {
+        --top;
+        if (sd[top] > H.wd32) continue;
+        int32_t x = sn[top];
+        if (x < 0) {
+          pending = x & 0x7fffffff;
+          continue;
+        }
+        if (st) st[0] += 1;
+        const float4* r2 = tv.pair + (int64_t)x * PF;
+        float llo[4 * NV], lhi[4 * NV], rlo[4 * NV], rhi[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 a = __ldg(&r2[h]), b = __ldg(&r2[NV + h]);
+          float4 c = __ldg(&r2[2 * NV + h]), d = __ldg(&r2[3 * NV + h]);
+          llo[4 * h] = a.x; llo[4 * h + 1] = a.y; llo[4 * h + 2] = a.z; llo[4 * h + 3] = a.w;
+          lhi[4 * h] = b.x; lhi[4 * h + 1] = b.y; lhi[4 * h + 2] = b.z; lhi[4 * h + 3] = b.w;
+          rlo[4 * h] = c.x; rlo[4 * h + 1] = c.y; rlo[4 * h + 2] = c.z; rlo[4 * h + 3] = c.w;
+          rhi[4 * h] = d.x; rhi[4 * h + 1] = d.y; rhi[4 * h + 2] = d.z; rhi[4 * h + 3] = d.w;
+        }
+        int4 xi = __ldg(reinterpret_cast<const int4*>(&r2[4 * NV]));
+        float ml = rec_mind_lb<D, PER>(tv, qs, llo, lhi);
+        float mr = rec_mind_lb<D, PER>(tv, qs, rlo, rhi);
+        int32_t L = xi.x | (xi.z ? (int32_t)0x80000000 : 0);
+        int32_t R = xi.y | (xi.w ? (int32_t)0x80000000 : 0);
+        bool nl = ml <= H.wd32, nr = mr <= H.wd32;
+        if (nl && nr) {
+          bool lf = ml <= mr;
+          sn[top] = lf ? R : L;
+          sd[top] = lf ? mr : ml;
+          sn[top + 1] = lf ? L : R;
+          sd[top + 1] = lf ? ml : mr;
+          top += 2;
+        } else if (nl || nr) {
+          sn[top] = nl ? L : R;
+          sd[top] = nl ? ml : mr;
+          top += 1;
+        }
+      } else {
+        if (parent < 0) {
+          done = true;
+          continue;
+        }
+        float r = sqrtf(H.wd32) * 1.0000003f;
+        const float* c32 = tv.cell32 + (int64_t)C * 2 * D;
+        bool inside = true;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float2 cl = __ldg(reinterpret_cast<const float2*>(c32) + j);
+          inside = inside && (qs.q32[j] - r - qs.dlt[j] >= cl.x) &&
+                   (qs.q32[j] + r + qs.dlt[j] <= cl.y);
+        }
+        if (inside) {
+          if (st) st[7] += 1;
+          done = true;
+          continue;
+        }
+        if (st) st[1] += 1;
+        const float4* rec = tv.pair + (int64_t)parent * PF;
+        int4 info = __ldg(reinterpret_cast<const int4*>(&rec[4 * NV]));
+        const int side = (info.x == C) ? 1 : 0;
+        float lo[4 * NV], hi[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 a = __ldg(&rec[side * 2 * NV + h]), b = __ldg(&rec[side * 2 * NV + NV + h]);
+          lo[4 * h] = a.x; lo[4 * h + 1] = a.y; lo[4 * h + 2] = a.z; lo[4 * h + 3] = a.w;
+          hi[4 * h] = b.x; hi[4 * h + 1] = b.y; hi[4 * h + 2] = b.z; hi[4 * h + 3] = b.w;
+        }
+        float ms = rec_mind_lb<D, PER>(tv, qs, lo, hi);
+        if (ms <= H.wd32) {
+          int32_t S = side ? info.y : info.x;
+          int sleaf = side ? info.w : info.z;
+          sn[0] = S | (sleaf ? (int32_t)0x80000000 : 0);
+          sd[0] = ms;
+          top = 1;
+        }
+        C = parent;
+        parent = load_meta(tv.meta, C).parent;
+      }
+    }
+    // ---- finished lanes order their heap; the warp writes those rows coalesced
+    const bool fin = active && done && pending < 0;
+    if (fin) {
+      lane_heap_finish(H);
+      if (sorted) lane_heap_sort(H);
+      active = false;
+    }
+    unsigned finm = __ballot_sync(0xffffffffu, fin);
+    if (finm) {
+      __syncwarp();
+      while (finm) {
+        const int src = __ffs(finm) - 1;
+        finm &= finm - 1;
+        const int64_t r = __shfl_sync(0xffffffffu, row, src);
+        const unsigned long long* rk = keys + src * KS + 1;
+        const int32_t* ri = ids + src * KS + 1;
+        for (int j = lane; j < k; j += 32) {
+          int32_t id = ri[j];
+          dist[r * k + j] = sqrt(__longlong_as_double((long long)rk[j]));
+          idx[r * k + j] = id < 0 ? -2 : (int64_t)id;
+        }
+      }
+      __syncwarp();
+    }
+    // ---- lanes holding a leaf scan together
+    if (pending >= 0) {
+      NodeMeta xm = load_meta(tv.meta, pending);
+      if (st) st[2] += 1;
+      lane_scan_leaf<D, PER>(tv, q, pending, xm.start, xm.count, H, st);
+      pending = -1;
+    }
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = stv[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+}
+
 // ------------------------------------------------------------ query order
 template <int D>
 __global__ void k_locate(const NodeMeta* __restrict__ meta, const double* __restrict__ Q,
-                         int64_t nq, int32_t* __restrict__ key, int32_t* __restrict__ hist) {
+                         int64_t nq, int32_t* __restrict__ key, int32_t* __restrict__ hist,
+                         int32_t* __restrict__ qleaf) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
   double q[D];
@@ -262,6 +1402,7 @@ __global__ void k_locate(const NodeMeta* __restrict__ meta, const double* __rest
     m = load_meta(meta, node);
   }
   key[i] = m.start;
+  if (qleaf) qleaf[i] = node;
   atomicAdd(&hist[m.start], 1);
 }
 
@@ -276,9 +1417,45 @@ __global__ void k_bucket_scatter(const int32_t* __restrict__ key, int64_t nq,
 }
 
 template <int D, bool PER>
-ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
-                      int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
+                      const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
+                      int64_t* idx, cudaStream_t s) {
   TreeView tv = t->view();
+  const int var = knn_variant();
+  if (k <= kSmemK && t->screen_ok && var == 5 && t->depth < kUpStack - 2) {
+    const int nwp = 4;
+    size_t sm = (size_t)nwp * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_persist<D, PER>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int dev = 0, sms = 0, per_sm = 0;
+    CKD_CUDA(cudaGetDevice(&dev));
+    CKD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CKD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_persist<D, PER>,
+                                                           nwp * 32, sm));
+    if (knn_blocks_per_sm() > 0) per_sm = std::min(per_sm, knn_blocks_per_sm());
+    int64_t grid = std::min<int64_t>((int64_t)std::max(1, per_sm) * sms, cdiv(cdiv(nq, 32), nwp));
+    unsigned long long* counter = nullptr;
+    CKD_CUDA(dev_alloc((void**)&counter, sizeof(unsigned long long), s));
+    CKD_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    k_knn_persist<D, PER><<<(unsigned)grid, nwp * 32, sm, s>>>(
+        tv, q, order, qleaf, nq, k, sorted, counter, dist, idx, knn_stats_buffer());
+    CKD_LAUNCH_CHECK();
+    CKD_CUDA(dev_free(counter, s));
+    return CKD_OK;
+  }
+  if (k <= kSmemK && t->screen_ok && var == 4 && t->depth < kUpStack - 2) {
+    const int nwu = knn_warps_per_block();
+    const int64_t blocks_u = cdiv(cdiv(nq, 32), nwu);
+    size_t sm = (size_t)nwu * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    const int bps = knn_blocks_per_sm();
+    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);  // cap residency via shared memory
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_up<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm));
+    k_knn_up<D, PER><<<(unsigned)blocks_u, nwu * 32, sm, s>>>(tv, q, order, qleaf, nq, k, sorted,
+                                                              dist, idx, knn_stats_buffer());
+    CKD_LAUNCH_CHECK();
+    return CKD_OK;
+  }
   const int threads = 128, nw = threads / 32;
   int64_t warps = cdiv(nq, 32);
   unsigned blocks = (unsigned)cdiv(warps, nw);
@@ -287,7 +1464,21 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order, 
   bool use_gstack = stack_len > kStack || k > kSmemK;
   if (use_gstack)
     CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
-  if (k <= kSmemK) {
+  if (k <= kSmemK && t->screen_ok && (var == 0 || var == 3) && t->depth < kLaneStack - 1) {
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm));
+    k_knn_lane<D, PER><<<blocks, threads, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
+                                                   knn_stats_buffer());
+  } else if (k <= kSmemK && t->screen_ok && var != 1) {
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t)) +
+                (use_gstack ? 0 : (size_t)nw * kStack * sizeof(int32_t));
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_screen<D, PER>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_knn_screen<D, PER><<<blocks, threads, sm, s>>>(tv, q, order, nq, k, sorted,
+                                                     use_gstack ? gstack : nullptr, stack_len,
+                                                     dist, idx, knn_stats_buffer());
+  } else if (k <= kSmemK) {
     size_t sm = (size_t)nw * k * 32 * (sizeof(double) + sizeof(int32_t)) +
                 (use_gstack ? 0 : (size_t)nw * kStack * sizeof(int32_t));
     CKD_CUDA(cudaFuncSetAttribute(k_knn_smem<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -305,15 +1496,16 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order, 
 }
 
 template <int D>
-ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq,
-                          int k, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
-  if (t->periodic) return knn_launch<D, true>(t, q, order, nq, k, sorted, dist, idx, s);
-  return knn_launch<D, false>(t, q, order, nq, k, sorted, dist, idx, s);
+ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* order,
+                          const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
+                          int64_t* idx, cudaStream_t s) {
+  if (t->periodic) return knn_launch<D, true>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+  return knn_launch<D, false>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
 }
 
 template <int D>
 ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                      cudaStream_t s) {
+                      int32_t* qleaf, cudaStream_t s) {
   int64_t n = t->n;
   int32_t *key = nullptr, *hist = nullptr, *off = nullptr;
   CKD_CUDA(dev_alloc((void**)&key, sizeof(int32_t) * nq, s));
@@ -321,7 +1513,7 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   CKD_CUDA(dev_alloc((void**)&off, sizeof(int32_t) * (n + 1), s));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   unsigned g = (unsigned)cdiv(nq, 256);
-  k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist);
+  k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist, qleaf);
   CKD_LAUNCH_CHECK();
   CKD_TRY(scan_i32(hist, off, n, s));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
@@ -335,48 +1527,75 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
 
 }  // namespace
 
+ckd_status knn_stats(int enable, int64_t* out) {
+  void* p = nullptr;
+  CKD_CUDA(cudaGetSymbolAddress(&p, g_knn_stats));
+  if (out) {
+    CKD_CUDA(cudaDeviceSynchronize());
+    CKD_CUDA(cudaMemcpy(out, p, sizeof(int64_t) * 8, cudaMemcpyDeviceToHost));
+  }
+  CKD_CUDA(cudaMemset(p, 0, sizeof(unsigned long long) * 8));
+  CKD_CUDA(cudaDeviceSynchronize());
+  g_stats_on = enable != 0;
+  return CKD_OK;
+}
+
 ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                       cudaStream_t s) {
+                       int32_t* qleaf, cudaStream_t s) {
   switch (t->d) {
-    case 1: return order_impl<1>(t, q, nq, order, s);
-    case 2: return order_impl<2>(t, q, nq, order, s);
-    case 3: return order_impl<3>(t, q, nq, order, s);
-    case 4: return order_impl<4>(t, q, nq, order, s);
-    case 5: return order_impl<5>(t, q, nq, order, s);
-    case 6: return order_impl<6>(t, q, nq, order, s);
-    case 7: return order_impl<7>(t, q, nq, order, s);
-    case 8: return order_impl<8>(t, q, nq, order, s);
+    case 1: return order_impl<1>(t, q, nq, order, qleaf, s);
+    case 2: return order_impl<2>(t, q, nq, order, qleaf, s);
+    case 3: return order_impl<3>(t, q, nq, order, qleaf, s);
+    case 4: return order_impl<4>(t, q, nq, order, qleaf, s);
+    case 5: return order_impl<5>(t, q, nq, order, qleaf, s);
+    case 6: return order_impl<6>(t, q, nq, order, qleaf, s);
+    case 7: return order_impl<7>(t, q, nq, order, qleaf, s);
+    case 8: return order_impl<8>(t, q, nq, order, qleaf, s);
   }
   return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+}
+
+ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
+                       cudaStream_t s) {
+  return query_order(t, q, nq, order, nullptr, s);
 }
 
 // Queries are ordered by leaf when there are enough of them to fill many warps.
 bool want_order(const ckd_tree* t, int64_t nq) { return nq >= 4096 && nq * 8 >= t->n / 64; }
 
-ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
-                       int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
+                       const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
+                       int64_t* idx, cudaStream_t s) {
   switch (t->d) {
-    case 1: return knn_dispatch_d<1>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 2: return knn_dispatch_d<2>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 3: return knn_dispatch_d<3>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 4: return knn_dispatch_d<4>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 5: return knn_dispatch_d<5>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 6: return knn_dispatch_d<6>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 7: return knn_dispatch_d<7>(t, q, order, nq, k, sorted, dist, idx, s);
-    case 8: return knn_dispatch_d<8>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 1: return knn_dispatch_d<1>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 2: return knn_dispatch_d<2>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 3: return knn_dispatch_d<3>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 4: return knn_dispatch_d<4>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 5: return knn_dispatch_d<5>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 6: return knn_dispatch_d<6>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 7: return knn_dispatch_d<7>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 8: return knn_dispatch_d<8>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
   }
   return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+}
+
+ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+  return knn_ordered(t, q, order, nullptr, nq, k, sorted, dist, idx, s);
 }
 
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s) {
   int32_t* order = nullptr;
+  int32_t* qleaf = nullptr;
   if (want_order(t, nq)) {
     CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
-    CKD_TRY(query_order(t, q, nq, order, s));
+    CKD_CUDA(dev_alloc((void**)&qleaf, sizeof(int32_t) * nq, s));
+    CKD_TRY(query_order(t, q, nq, order, qleaf, s));
   }
-  ckd_status st = knn_ordered(t, q, order, nq, k, sorted, dist, idx, s);
+  ckd_status st = knn_ordered(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
   if (order) dev_free(order, s);
+  if (qleaf) dev_free(qleaf, s);
   return st;
 }
 

@@ -96,6 +96,27 @@ ckd_status ckd_knn_ordered(const ckd_tree* tree, const double* q_dev, int64_t nq
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t ckd_launch_count(void);
 
+/* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (the
+ * FP32-screened kernel when k <= 64 and coordinates allow it), 1 = FP64-only
+ * traversal, 2 = FP32-screened whenever possible.  Every variant returns the same
+ * exact result. */
+ckd_status ckd_set_knn_variant(int variant);
+
+/* Process-wide launch tuning of the search kernels (no reference counterpart;
+ * set by the autotuner).  key 0: kNN variant (as ckd_set_knn_variant);
+ * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
+ * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
+ * of the kNN kernel (1..8, default 4). */
+ckd_status ckd_set_tuning(int key, int value);
+
+/* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference
+ * counterpart).  Copies the counters accumulated since the previous call into
+ * out8 (if not NULL; 8 entries: node pops, needed pops, leaf visits, points
+ * screened, warp insert rounds, FP64 evaluations, heap inserts, lanes active on
+ * leaf visits), clears them, and turns collection on (enable=1) or off.
+ * Synchronises the device. */
+ckd_status ckd_knn_stats(int enable, int64_t* out8);
+
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);

@@ -108,8 +108,16 @@ KNN_CASES = [
 ]
 
 
+@pytest.fixture(params=[1, 2, 3, 4, 5], ids=["fp64", "screened", "lane", "bottom_up", "persistent"])
+def knn_variant(request, gpu):
+    from cosmokdtree_b200 import _lib
+    _lib.check(_lib.load().ckd_set_knn_variant(request.param))
+    yield request.param
+    _lib.load().ckd_set_knn_variant(0)
+
+
 @pytest.mark.parametrize("name,n,d,periodic,leaf,nq,k", KNN_CASES)
-def test_gpu_knn_matches_oracle(gpu, oracle, name, n, d, periodic, leaf, nq, k):
+def test_gpu_knn_matches_oracle(gpu, oracle, knn_variant, name, n, d, periodic, leaf, nq, k):
     P = make_points(name, n, d, periodic)
     rng = np.random.default_rng(99)
     Q = np.concatenate([P[rng.integers(0, n, nq // 2)],
