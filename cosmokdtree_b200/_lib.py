@@ -83,6 +83,8 @@ SIGNATURES = {
     "ckd_launch_count": [],
     "ckd_set_knn_variant": [_int],
     "ckd_set_tuning": [_int, _int],
+    "ckd_set_kernel_timing": [_int],
+    "ckd_kernel_ms": [ctypes.POINTER(ctypes.c_float)],
     "ckd_knn_stats": [_int, _pi64],
     "ckd_ball_count": [_vp, _vp, _i64, _dbl, _vp, _vp],
     "ckd_ball_fill": [_vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],

@@ -34,7 +34,27 @@ int knn_variant() { return g_knn_variant.load(std::memory_order_relaxed); }
 static std::atomic<int> g_knn_bps{0}, g_knn_wpb{4};
 int knn_blocks_per_sm() { return g_knn_bps.load(std::memory_order_relaxed); }
 int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
+void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ------------------------------------------------------------ kernel timing
+static std::atomic<int> g_timing{0};
+static cudaEvent_t g_ev[2];
+static bool g_ev_ok = false, g_ev_recorded = false;
+void timing_begin(cudaStream_t s) {
+  if (!g_timing.load()) return;
+  if (!g_ev_ok) {
+    cudaEventCreate(&g_ev[0]);
+    cudaEventCreate(&g_ev[1]);
+    g_ev_ok = true;
+  }
+  cudaEventRecord(g_ev[0], s);
+}
+void timing_end(cudaStream_t s) {
+  if (!g_timing.load() || !g_ev_ok) return;
+  cudaEventRecord(g_ev[1], s);
+  g_ev_recorded = true;
+}
 
 // ---------------------------------------------------------- scratch memory
 // One stream-ordered pool per device, keeping freed blocks cached.
@@ -287,8 +307,22 @@ int64_t ckd_launch_count(void) { return g_launches.load(); }
 ckd_status ckd_knn_stats(int enable, int64_t* out8) { return knn_stats(enable, out8); }
 
 ckd_status ckd_set_knn_variant(int variant) {
-  if (variant < 0 || variant > 5) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..5");
+  if (variant < 0 || variant > 6) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..6");
   g_knn_variant.store(variant);
+  return CKD_OK;
+}
+
+ckd_status ckd_set_kernel_timing(int enable) {
+  g_timing.store(enable ? 1 : 0);
+  return CKD_OK;
+}
+
+ckd_status ckd_kernel_ms(float* ms) {
+  if (!ms) return fail(CKD_ERR_BAD_ARG, "null output");
+  *ms = -1.0f;
+  if (!g_ev_recorded) return CKD_OK;
+  CKD_CUDA(cudaEventSynchronize(g_ev[1]));
+  CKD_CUDA(cudaEventElapsedTime(ms, g_ev[0], g_ev[1]));
   return CKD_OK;
 }
 
@@ -302,6 +336,10 @@ ckd_status ckd_set_tuning(int key, int value) {
     case 2:
       if (value < 1 || value > 8) return fail(CKD_ERR_BAD_ARG, "warps per block must be 1..8");
       g_knn_wpb.store(value);
+      return CKD_OK;
+    case 3:
+      if (value < 10 || value > 1000) return fail(CKD_ERR_BAD_ARG, "bucket radius factor must be 10..1000");
+      set_knn_bucket_alpha(value / 100.0f);
       return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");

@@ -42,6 +42,10 @@ int knn_variant();
 int knn_blocks_per_sm();
 int knn_warps_per_block();
 
+// events bracketing the main search kernel when kernel timing is on
+void timing_begin(cudaStream_t s);
+void timing_end(cudaStream_t s);
+
 // stream-ordered scratch allocation from a per-device pool
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t dev_free(void* p, cudaStream_t s);

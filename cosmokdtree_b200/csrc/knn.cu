@@ -21,6 +21,11 @@ namespace ckd {
 namespace {
 
 constexpr int kStack = 96;   // per-warp traversal stack in shared memory
+float knn_bucket_alpha_v = 1.5f;
+float knn_bucket_alpha() { return knn_bucket_alpha_v; }
+}  // namespace
+void set_knn_bucket_alpha(float a) { knn_bucket_alpha_v = a; }
+namespace {
 
 // process-wide traversal statistics of the screened kernel (diagnostics)
 __device__ unsigned long long g_knn_stats[8];
@@ -1381,6 +1386,342 @@ __global__ void __launch_bounds__(128) k_knn_persist(TreeView tv, const double* 
   }
 }
 
+// ========================================== warp-per-bucket search (v6)
+// Queries that fall in the same leaf form a bucket; one warp serves a bucket of
+// up to 32 queries with regular, fully lane-parallel loops:
+//  1. a bucket radius R is guessed from the local density (the nearest ancestor
+//     holding at least 2k points);
+//  2. every leaf whose FP32 box lies within R of the bucket's bounding box is
+//     collected by a warp-parallel frontier walk from the root, and the point
+//     indices of those leaves form the candidate list (shared memory);
+//  3. for each query the warp streams the candidates (one per lane, exact FP64
+//     squared distance with the reference arithmetic) into a warp-wide sorted
+//     top-32 list (lane j holds rank j): candidates that rank before the current
+//     32nd are compacted into a pending buffer, and every 32 pending entries are
+//     bitonic-sorted and bitonic-merged into the list;
+//  4. every point outside the candidate list is farther than R from every query
+//     of the bucket, so the list is exact iff its k-th squared distance is <= R^2
+//     (or the list covers the whole tree).  Unresolved queries retry with 2R, up
+//     to kBucketRounds rounds; the rest go to a fallback list that the per-lane
+//     kernel finishes.
+constexpr int kBucketCmax = 1536;   // candidate points per bucket
+constexpr int kBucketFmax = 384;    // frontier capacity
+constexpr int kBucketRounds = 4;
+
+struct KV {
+  unsigned long long k;
+  int32_t i;
+};
+
+__device__ __forceinline__ bool kv_lt(unsigned long long ka, int32_t ia, unsigned long long kb,
+                                      int32_t ib) {
+  return ka < kb || (ka == kb && ia < ib);
+}
+
+// one compare-exchange stage of a bitonic network across the warp
+__device__ __forceinline__ void bitonic_step(unsigned long long& key, int32_t& id, int stride,
+                                             bool ascending_block) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long ok = __shfl_xor_sync(0xffffffffu, key, stride);
+  int32_t oi = __shfl_xor_sync(0xffffffffu, id, stride);
+  bool lower = (lane & stride) == 0;
+  bool other_smaller = kv_lt(ok, oi, key, id);
+  // the lower lane keeps the smaller element in an ascending block
+  bool take = (lower == ascending_block) ? other_smaller : !other_smaller && !(ok == key && oi == id);
+  if (take) {
+    key = ok;
+    id = oi;
+  }
+}
+
+__device__ __forceinline__ void bitonic_sort32(unsigned long long& key, int32_t& id) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+    bool asc = (lane & size) == 0 || size == 32;
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) bitonic_step(key, id, stride, asc);
+  }
+}
+
+// merge an ascending 32-list (tk, ti) with an ascending 32-list (pk, pi), keep the
+// 32 smallest, ascending
+__device__ __forceinline__ void merge_top32(unsigned long long& tk, int32_t& ti,
+                                            unsigned long long pk, int32_t pi) {
+  unsigned long long rk = __shfl_xor_sync(0xffffffffu, pk, 31);
+  int32_t ri = __shfl_xor_sync(0xffffffffu, pi, 31);
+  if (kv_lt(rk, ri, tk, ti)) {
+    tk = rk;
+    ti = ri;
+  }
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) bitonic_step(tk, ti, stride, true);
+}
+
+template <int D, bool PER>
+__device__ __forceinline__ float boxbox_gap_lb(const TreeView& tv, const float (&blo)[D],
+                                               const float (&bhi)[D], const float* nb,
+                                               const float (&dlt)[D]) {
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float2 lh = __ldg(reinterpret_cast<const float2*>(nb) + j);
+    float g = fmaxf(fmaxf(lh.x - bhi[j], blo[j] - lh.y), 0.0f);
+    if (PER && g > 0.0f) {
+      float L = (float)tv.L[j];
+      float wrapg = L - (fmaxf(bhi[j], lh.y) - fminf(blo[j], lh.x));
+      g = fminf(g, fmaxf(wrapg, 0.0f));
+    }
+    g = fmaxf(g - dlt[j], 0.0f);
+    s = fmaf(g, g, s);
+  }
+  return s * kShrink;
+}
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_knn_bucket(TreeView tv, const double* __restrict__ Q,
+                                                    const int32_t* __restrict__ order,
+                                                    const int4* __restrict__ buckets,
+                                                    int64_t nbuckets, int k, float alpha,
+                                                    double* __restrict__ dist,
+                                                    int64_t* __restrict__ idx,
+                                                    int32_t* __restrict__ fallback,
+                                                    unsigned int* __restrict__ nfallback,
+                                                    int64_t fallback_cap,
+                                                    unsigned long long* __restrict__ stats) {
+  __shared__ int32_t s_cand[4][kBucketCmax];
+  __shared__ int32_t s_front[4][2][kBucketFmax];
+  __shared__ unsigned long long s_pk[4][64];
+  __shared__ int32_t s_pi[4][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
+  const unsigned lt_mask = (1u << lane) - 1;
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int32_t* cand = s_cand[w];
+  for (int64_t b = (int64_t)blockIdx.x * 4 + w; b < nbuckets; b += (int64_t)gridDim.x * 4) {
+    const int4 bk = buckets[b];  // {first slot in order, queries, leaf, 0}
+    const int m = bk.y;
+    const bool has_q = lane < m;
+    const int64_t qi = has_q ? (int64_t)order[bk.x + lane] : 0;
+    double q[D];
+    float blo[D], bhi[D], dlt[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      q[j] = has_q ? Q[qi * D + j] : 0.0;
+      float lo = has_q ? __double2float_rd(q[j]) : FLT_MAX;
+      float hi = has_q ? __double2float_ru(q[j]) : -FLT_MAX;
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      }
+      blo[j] = lo;
+      bhi[j] = hi;
+      dlt[j] = kTwoM21 * (fmaxf(fabsf(lo), fabsf(hi)) + tv.slack[j]) * 1.0001f;
+    }
+    // ---- density radius from the nearest ancestor with >= 2k points
+    float R;
+    {
+      int32_t A = bk.z;
+      NodeMeta am = load_meta(tv.meta, A);
+      while (am.count < 2 * k && am.parent >= 0) {
+        A = am.parent;
+        am = load_meta(tv.meta, A);
+      }
+      const float* ab = tv.box32 + (int64_t)A * 2 * D;
+      float side[D], smax = 0.0f;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        float2 lh = __ldg(reinterpret_cast<const float2*>(ab) + j);
+        side[j] = lh.y - lh.x;
+        smax = fmaxf(smax, side[j]);
+      }
+      float lv = 0.0f;  // log volume with degenerate sides floored
+#pragma unroll
+      for (int j = 0; j < D; ++j) lv += __logf(fmaxf(side[j], 1e-3f * smax + 1e-30f));
+      // volume of the k-ball at the ancestor's density, unit-ball volume ~ 4 for d = 3
+      float lr = (__logf((float)k / (float)am.count) + lv - __logf(4.0f)) / (float)D;
+      R = alpha * __expf(lr);
+      if (!(R > 0.0f) || !(R < FLT_MAX)) R = smax + 1e-30f;
+    }
+    unsigned unresolved = __ballot_sync(0xffffffffu, has_q);
+    for (int round = 0; round < kBucketRounds && unresolved; ++round, R *= 2.0f) {
+      // ---- candidate leaves within R of the bucket box (frontier walk)
+      const float R2 = R * R;
+      int nf = 1, cur = 0, nc = 0;
+      bool overflow = false, all_leaves = true;
+      if (lane == 0) s_front[w][0][0] = 0;
+      __syncwarp();
+      while (nf > 0 && !overflow) {
+        int nn = 0;
+        for (int base = 0; base < nf; base += 32) {
+          const int fi = base + lane;
+          int32_t node = fi < nf ? s_front[w][cur][fi] : -1;
+          bool need = false, leaf = false;
+          NodeMeta nm;
+          if (node >= 0) {
+            if (st) st[0] += 1;
+            need = boxbox_gap_lb<D, PER>(tv, blo, bhi, tv.box32 + (int64_t)node * 2 * D, dlt) <= R2;
+            nm = load_meta(tv.meta, node);
+            leaf = nm.left < 0;
+            if (!need) all_leaves = false;
+          }
+          // internal: both children to the next frontier
+          unsigned im = __ballot_sync(0xffffffffu, need && !leaf);
+          int ipos = nn + 2 * __popc(im & lt_mask);
+          if (need && !leaf && ipos + 1 < kBucketFmax) {
+            s_front[w][1 - cur][ipos] = nm.left;
+            s_front[w][1 - cur][ipos + 1] = nm.left + 1;
+          }
+          nn += 2 * __popc(im);
+          if (nn > kBucketFmax) overflow = true;
+          // leaves: append their points
+          unsigned lm = __ballot_sync(0xffffffffu, need && leaf);
+          while (lm) {
+            const int src = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int32_t s0 = __shfl_sync(0xffffffffu, nm.start, src);
+            const int32_t c0 = __shfl_sync(0xffffffffu, nm.count, src);
+            if (nc + c0 > kBucketCmax) {
+              overflow = true;
+            } else {
+              for (int i = lane; i < c0; i += 32) cand[nc + i] = s0 + i;
+              nc += c0;
+            }
+          }
+        }
+        __syncwarp();
+        nf = nn;
+        cur = 1 - cur;
+      }
+      // every lane must agree: a node pruned by any lane means the list is partial
+      all_leaves = __all_sync(0xffffffffu, all_leaves);
+      if (overflow) break;
+      __syncwarp();
+      if (st) st[1] += nc;
+      // ---- each unresolved query: stream the candidates into a warp top-32
+      unsigned todo = unresolved;
+      while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        double qq[D];
+#pragma unroll
+        for (int j = 0; j < D; ++j) qq[j] = __shfl_sync(0xffffffffu, q[j], src);
+        unsigned long long tk = kHugeKey;  // lane j holds rank j
+        int32_t ti = -1;
+        unsigned long long mk = kHugeKey;  // current 32nd
+        int32_t mi = -1;
+        int np = 0;
+        for (int base = 0; base < nc; base += 32) {
+          const int c = base + lane;
+          unsigned long long key = kHugeKey;
+          int32_t id = -1;
+          bool pass = false;
+          if (c < nc) {
+            const int32_t p = cand[c];
+            double d2 = point_d2<D, PER>(tv, qq, p);
+            key = (unsigned long long)__double_as_longlong(d2);
+            if (key < mk || key == mk) {
+              id = __ldg(&tv.ids[p]);
+              pass = kv_lt(key, id, mk, mi);
+            }
+          }
+          unsigned pm = __ballot_sync(0xffffffffu, pass);
+          if (pass) {
+            const int pos = np + __popc(pm & lt_mask);
+            s_pk[w][pos] = key;
+            s_pi[w][pos] = id;
+          }
+          np += __popc(pm);
+          if (st) st[2] += __popc(pm);
+          __syncwarp();
+          if (np >= 32) {
+            unsigned long long pk = s_pk[w][lane];
+            int32_t pi = s_pi[w][lane];
+            __syncwarp();
+            if (lane < np - 32) {  // keep the overflow for the next merge
+              s_pk[w][lane] = s_pk[w][lane + 32];
+              s_pi[w][lane] = s_pi[w][lane + 32];
+            }
+            np -= 32;
+            bitonic_sort32(pk, pi);
+            merge_top32(tk, ti, pk, pi);
+            mk = __shfl_sync(0xffffffffu, tk, 31);
+            mi = __shfl_sync(0xffffffffu, ti, 31);
+            if (st) st[3] += 1;
+            __syncwarp();
+          }
+        }
+        if (np > 0) {
+          unsigned long long pk = lane < np ? s_pk[w][lane] : kHugeKey;
+          int32_t pi = lane < np ? s_pi[w][lane] : -1;
+          __syncwarp();
+          bitonic_sort32(pk, pi);
+          merge_top32(tk, ti, pk, pi);
+          if (st) st[3] += 1;
+        }
+        // exact iff the k-th is within the radius the leaves were gathered with
+        // (every point left out has a larger squared distance), or the
+        // candidates cover the whole tree
+        const unsigned long long kk = __shfl_sync(0xffffffffu, tk, k - 1);
+        const double r2d = (double)R2;
+        const bool ok = all_leaves || (kk != kHugeKey && kk <= (unsigned long long)__double_as_longlong(r2d));
+        if (ok) {
+          const int64_t row = __shfl_sync(0xffffffffu, qi, src);
+          if (lane < k) {
+            dist[row * k + lane] = sqrt(__longlong_as_double((long long)tk));
+            idx[row * k + lane] = ti < 0 ? -2 : (int64_t)ti;
+          }
+          unresolved &= ~(1u << src);
+        }
+      }
+    }
+    // ---- leftovers go to the fallback list
+    if (unresolved) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(nfallback, (unsigned)__popc(unresolved));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      const int64_t pos = (int64_t)base + __popc(unresolved & lt_mask);
+      if (((unresolved >> lane) & 1u) && pos < fallback_cap) fallback[pos] = (int32_t)qi;
+      if (st) st[4] += __popc(unresolved);
+    }
+    __syncwarp();
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = st[c];
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+}
+
+// bucket list: for every leaf holding queries, ceil(count / 32) buckets
+__global__ void k_bucket_count(const NodeMeta* __restrict__ meta, int32_t n_nodes,
+                               const int32_t* __restrict__ off, int32_t* __restrict__ nb) {
+  int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n_nodes) return;
+  NodeMeta m = meta[a];
+  int c = 0;
+  if (m.left < 0) {
+    int32_t cnt = off[m.start + 1] - off[m.start];
+    c = (cnt + 31) / 32;
+  }
+  nb[a] = c;
+}
+
+__global__ void k_bucket_emit(const NodeMeta* __restrict__ meta, int32_t n_nodes,
+                              const int32_t* __restrict__ off, const int32_t* __restrict__ nbo,
+                              int4* __restrict__ buckets) {
+  int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n_nodes) return;
+  NodeMeta m = meta[a];
+  if (m.left >= 0) return;
+  int32_t b0 = off[m.start], cnt = off[m.start + 1] - b0;
+  int32_t o = nbo[a];
+  for (int c = 0; c * 32 < cnt; ++c)
+    buckets[o + c] = make_int4(b0 + 32 * c, min(32, cnt - 32 * c), a, 0);
+}
+
 // ------------------------------------------------------------ query order
 template <int D>
 __global__ void k_locate(const NodeMeta* __restrict__ meta, const double* __restrict__ Q,
@@ -1419,9 +1760,17 @@ __global__ void k_bucket_scatter(const int32_t* __restrict__ key, int64_t nq,
 template <int D, bool PER>
 ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
                       const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
-                      int64_t* idx, cudaStream_t s) {
+                      int64_t* idx, cudaStream_t s, int force_variant = -1) {
   TreeView tv = t->view();
-  const int var = knn_variant();
+  const int var = force_variant >= 0 ? force_variant : knn_variant();
+  if (force_variant < 0) timing_begin(s);
+  struct TimingEnd {
+    cudaStream_t s;
+    bool on;
+    ~TimingEnd() {
+      if (on) timing_end(s);
+    }
+  } timing_guard{s, force_variant < 0};
   if (k <= kSmemK && t->screen_ok && var == 5 && t->depth < kUpStack - 2) {
     const int nwp = 4;
     size_t sm = (size_t)nwp * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
@@ -1505,7 +1854,7 @@ ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* ord
 
 template <int D>
 ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                      int32_t* qleaf, cudaStream_t s) {
+                      int32_t* qleaf, cudaStream_t s, int32_t** off_out = nullptr) {
   int64_t n = t->n;
   int32_t *key = nullptr, *hist = nullptr, *off = nullptr;
   CKD_CUDA(dev_alloc((void**)&key, sizeof(int32_t) * nq, s));
@@ -1521,8 +1870,62 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   CKD_LAUNCH_CHECK();
   CKD_CUDA(dev_free(key, s));
   CKD_CUDA(dev_free(hist, s));
-  CKD_CUDA(dev_free(off, s));
+  if (off_out)
+    *off_out = off;
+  else
+    CKD_CUDA(dev_free(off, s));
   return CKD_OK;
+}
+
+// Warp-per-bucket search: locate + counting sort, bucket list, bucket kernel,
+// then the per-lane kernel for any query the bucket rounds left unresolved.
+template <int D, bool PER>
+ckd_status bucket_run(const ckd_tree* t, const double* q, int64_t nq, int k, double* dist,
+                      int64_t* idx, cudaStream_t s) {
+  int32_t *order = nullptr, *off = nullptr, *nb = nullptr, *nbo = nullptr, *fb = nullptr;
+  unsigned int* nfb = nullptr;
+  int4* buckets = nullptr;
+  const int32_t nn = t->n_nodes;
+  CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
+  CKD_TRY(order_impl<D>(t, q, nq, order, nullptr, s, &off));
+  CKD_CUDA(dev_alloc((void**)&nb, sizeof(int32_t) * nn, s));
+  CKD_CUDA(dev_alloc((void**)&nbo, sizeof(int32_t) * (nn + 1), s));
+  k_bucket_count<<<(unsigned)cdiv(nn, 256), 256, 0, s>>>(t->meta, nn, off, nb);
+  CKD_LAUNCH_CHECK();
+  CKD_TRY(scan_i32(nb, nbo, nn, s));
+  int32_t nbuckets = 0;
+  CKD_CUDA(cudaMemcpyAsync(&nbuckets, nbo + nn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CKD_CUDA(cudaStreamSynchronize(s));
+  CKD_CUDA(dev_alloc((void**)&buckets, sizeof(int4) * std::max(1, nbuckets), s));
+  k_bucket_emit<<<(unsigned)cdiv(nn, 256), 256, 0, s>>>(t->meta, nn, off, nbo, buckets);
+  CKD_LAUNCH_CHECK();
+  CKD_CUDA(dev_alloc((void**)&fb, sizeof(int32_t) * nq, s));
+  CKD_CUDA(dev_alloc((void**)&nfb, sizeof(unsigned int), s));
+  CKD_CUDA(cudaMemsetAsync(nfb, 0, sizeof(unsigned int), s));
+  TreeView tv = t->view();
+  int dev = 0, sms = 0, per_sm = 0;
+  CKD_CUDA(cudaGetDevice(&dev));
+  CKD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CKD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_bucket<D, PER>, 128, 0));
+  int64_t grid = std::min<int64_t>((int64_t)std::max(1, per_sm) * sms * 4, cdiv(nbuckets, 4));
+  if (nbuckets > 0) {
+    timing_begin(s);
+    k_knn_bucket<D, PER><<<(unsigned)std::max<int64_t>(1, grid), 128, 0, s>>>(
+        tv, q, order, buckets, nbuckets, k, knn_bucket_alpha(), dist, idx, fb, nfb, nq,
+        knn_stats_buffer());
+    CKD_LAUNCH_CHECK();
+    timing_end(s);
+  }
+  unsigned int nfallback = 0;
+  CKD_CUDA(cudaMemcpyAsync(&nfallback, nfb, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  CKD_CUDA(cudaStreamSynchronize(s));
+  if ((int64_t)nfallback > nq) return fail(CKD_ERR_CUDA, "internal error: fallback list overflow");
+  ckd_status st = CKD_OK;
+  if (nfallback > 0) st = knn_launch<D, PER>(t, q, fb, nullptr, nfallback, k, 1, dist, idx, s, 3);
+  for (void* p : {(void*)order, (void*)off, (void*)nb, (void*)nbo, (void*)fb, (void*)nfb,
+                  (void*)buckets})
+    dev_free(p, s);
+  return st;
 }
 
 }  // namespace
@@ -1584,8 +1987,22 @@ ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
   return knn_ordered(t, q, order, nullptr, nq, k, sorted, dist, idx, s);
 }
 
+bool use_bucket(const ckd_tree* t, int64_t nq, int k) {
+  const int var = knn_variant();
+  return var == 6 && k <= 32 && t->screen_ok && want_order(t, nq);
+}
+
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s) {
+  if (use_bucket(t, nq, k)) {
+    switch (t->d * 2 + (t->periodic ? 1 : 0)) {
+#define CKD_BK(DD)                                                           \
+  case 2 * DD: return bucket_run<DD, false>(t, q, nq, k, dist, idx, s);      \
+  case 2 * DD + 1: return bucket_run<DD, true>(t, q, nq, k, dist, idx, s);
+      CKD_BK(1) CKD_BK(2) CKD_BK(3) CKD_BK(4) CKD_BK(5) CKD_BK(6) CKD_BK(7) CKD_BK(8)
+#undef CKD_BK
+    }
+  }
   int32_t* order = nullptr;
   int32_t* qleaf = nullptr;
   if (want_order(t, nq)) {

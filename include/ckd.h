@@ -106,7 +106,8 @@ ckd_status ckd_set_knn_variant(int variant);
  * set by the autotuner).  key 0: kNN variant (as ckd_set_knn_variant);
  * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
  * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
- * of the kNN kernel (1..8, default 4). */
+ * of the kNN kernel (1..8, default 4); key 3: radius factor of the warp-per-bucket
+ * kNN search in hundredths (default 150 = 1.5x the density estimate). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference
@@ -116,6 +117,13 @@ ckd_status ckd_set_tuning(int key, int value);
  * leaf visits), clears them, and turns collection on (enable=1) or off.
  * Synchronises the device. */
 ckd_status ckd_knn_stats(int enable, int64_t* out8);
+
+/* Kernel timing (diagnostics, no reference counterpart).  With enable=1 the kNN
+ * entry points record CUDA events around their main search kernel on the
+ * caller's stream; ckd_kernel_ms waits for the last recorded pair and returns
+ * its elapsed milliseconds (or -1 if none was recorded). */
+ckd_status ckd_set_kernel_timing(int enable);
+ckd_status ckd_kernel_ms(float* ms);
 
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,

@@ -108,7 +108,8 @@ KNN_CASES = [
 ]
 
 
-@pytest.fixture(params=[1, 2, 3, 4, 5], ids=["fp64", "screened", "lane", "bottom_up", "persistent"])
+@pytest.fixture(params=[1, 2, 3, 4, 5, 6],
+                ids=["fp64", "screened", "lane", "bottom_up", "persistent", "bucket"])
 def knn_variant(request, gpu):
     from cosmokdtree_b200 import _lib
     _lib.check(_lib.load().ckd_set_knn_variant(request.param))
