@@ -102,6 +102,8 @@ ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
 ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
                        cudaStream_t s);
 ckd_status knn_stats(int enable, int64_t* out);
+ckd_status knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                       double* dist, int64_t* idx, cudaStream_t s);
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s);
@@ -343,6 +345,16 @@ ckd_status ckd_set_tuning(int key, int value) {
       return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
+}
+
+ckd_status ckd_knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                           double* dist, int64_t* idx, void* stream) {
+  CKD_TRY(check_tree(t));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  return knn_noalloc(t, q, nq, k, sorted, dist, idx, (cudaStream_t)stream);
 }
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,

@@ -11,6 +11,7 @@
 // caller's output rows.  Distances are FP64, separately rounded, so results are
 // bit-identical to the CPU restatement.
 #include <algorithm>
+#include <mutex>
 
 #include "ckd_common.cuh"
 #include "ckd_scan.cuh"
@@ -2014,6 +2015,153 @@ ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int so
   if (order) dev_free(order, s);
   if (qleaf) dev_free(qleaf, s);
   return st;
+}
+
+// ===================================================================
+// kNN without any device allocation (ckd_knn_noalloc)
+//
+// For callers that cannot allocate device memory during a search: host
+// applications that reserve all device memory up front and hand nothing to the
+// CUDA allocator afterwards, or latency-critical loops that cannot afford the
+// implicit synchronisation of an allocation.  The query-ordering scratch of the
+// search (per-query keys and the processing order, a histogram of coarse leaf
+// bins and its prefix sums) lives in one file-scope device array instead of
+// pool allocations; the search kernel itself needs only shared memory.
+//
+// Limits: at most kNoAllocMaxQ queries per call, k <= 64, tree depth < 92.
+// Every call shares the array, so calls whose work overlaps on the GPU (two
+// streams, or two host threads) race on it and must be serialised by the
+// caller.  The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, with that device current); make that first call
+// before any stream capture.  The array holds ~18 MB on every device that
+// loads the library, until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxQ = int64_t(1) << 21;  // queries per call
+constexpr int kNoAllocBins = 1 << 18;              // coarse leaf bins
+constexpr size_t kNoAllocBytes =
+    sizeof(int32_t) * (2 * (size_t)kNoAllocMaxQ + 2 * (size_t)kNoAllocBins + 64);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {nullptr};
+
+// host address of the scratch array on the current device (set up once per device)
+ckd_status noalloc_scratch(void** out) {
+  int dev = 0;
+  CKD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(CKD_ERR_NO_DEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return CKD_OK;
+}
+
+// leaf of each query, binned coarsely by the leaf's first point
+template <int D>
+__global__ void k_locate_bins(const NodeMeta* __restrict__ meta, const double* __restrict__ Q,
+                              int64_t nq, int shift, int32_t* __restrict__ key,
+                              int32_t* __restrict__ hist) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  double q[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) q[j] = Q[i * D + j];
+  NodeMeta m = load_meta(meta, 0);
+  while (m.left >= 0) {
+    double qa = 0.0;
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      if (j == m.axis) qa = q[j];
+    m = load_meta(meta, qa < m.split ? m.left : m.left + 1);
+  }
+  int32_t b = m.start >> shift;
+  key[i] = b;
+  atomicAdd(&hist[b], 1);
+}
+
+// exclusive scan of n <= kNoAllocBins counts by one block (out[n] = total)
+__global__ void __launch_bounds__(1024) k_scan_one_block(const int32_t* __restrict__ in, int n,
+                                                         int32_t* __restrict__ out) {
+  __shared__ int32_t tmp[32];
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+  int32_t s = 0;
+  for (int i = b0; i < b1; ++i) s += in[i];
+  int32_t tot;
+  int32_t pre = block_exclusive_scan<int32_t, 1024>(s, tmp, tot);
+  for (int i = b0; i < b1; ++i) {
+    int32_t v = in[i];
+    out[i] = pre;
+    pre += v;
+  }
+  if (threadIdx.x == 0) out[n] = tot;
+}
+
+template <int D, bool PER>
+ckd_status knn_noalloc_impl(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                            double* dist, int64_t* idx, cudaStream_t s) {
+  void* base = nullptr;
+  CKD_TRY(noalloc_scratch(&base));
+  int32_t* order = reinterpret_cast<int32_t*>(base);
+  int32_t* key = order + kNoAllocMaxQ;
+  int32_t* hist = key + kNoAllocMaxQ;
+  int32_t* off = hist + kNoAllocBins;
+  int shift = 0;
+  while ((t->n >> shift) >= kNoAllocBins) ++shift;
+  const int nbins = (int)((t->n >> shift) + 1);
+  CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * nbins, s));
+  const unsigned g = (unsigned)cdiv(nq, 256);
+  k_locate_bins<D><<<g, 256, 0, s>>>(t->meta, q, nq, shift, key, hist);
+  CKD_LAUNCH_CHECK();
+  k_scan_one_block<<<1, 1024, 0, s>>>(hist, nbins, off);
+  CKD_LAUNCH_CHECK();
+  CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * nbins, s));
+  k_bucket_scatter<<<g, 256, 0, s>>>(key, nq, off, hist, order);
+  CKD_LAUNCH_CHECK();
+  TreeView tv = t->view();
+  const int nw = 4;
+  const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+  if (t->screen_ok && t->depth < kLaneStack - 1) {
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm));
+    k_knn_lane<D, PER><<<blocks, nw * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx, nullptr);
+  } else {
+    size_t sm = (size_t)nw * k * 32 * (sizeof(double) + sizeof(int32_t)) +
+                (size_t)nw * kStack * sizeof(int32_t);
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_smem<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm));
+    k_knn_smem<D, PER><<<blocks, nw * 32, sm, s>>>(tv, q, order, nq, k, sorted, nullptr, kStack,
+                                                   dist, idx);
+  }
+  CKD_LAUNCH_CHECK();
+  return CKD_OK;
+}
+
+}  // namespace
+
+ckd_status knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                       double* dist, int64_t* idx, cudaStream_t s) {
+  if (nq > kNoAllocMaxQ)
+    return fail(CKD_ERR_BAD_ARG, "ckd_knn_noalloc: at most 2097152 queries per call");
+  if (k > kSmemK) return fail(CKD_ERR_BAD_ARG, "ckd_knn_noalloc: k must be <= 64");
+  if (t->depth >= kStack - 4)
+    return fail(CKD_ERR_BAD_ARG, "ckd_knn_noalloc: tree deeper than 91 levels");
+  switch (t->d * 2 + (t->periodic ? 1 : 0)) {
+#define CKD_NA(DD)                                                                     \
+  case 2 * DD: return knn_noalloc_impl<DD, false>(t, q, nq, k, sorted, dist, idx, s); \
+  case 2 * DD + 1: return knn_noalloc_impl<DD, true>(t, q, nq, k, sorted, dist, idx, s);
+    CKD_NA(1) CKD_NA(2) CKD_NA(3) CKD_NA(4) CKD_NA(5) CKD_NA(6) CKD_NA(7) CKD_NA(8)
+#undef CKD_NA
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
 }
 
 }  // namespace ckd

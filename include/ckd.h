@@ -125,6 +125,22 @@ ckd_status ckd_knn_stats(int enable, int64_t* out8);
 ckd_status ckd_set_kernel_timing(int enable);
 ckd_status ckd_kernel_ms(float* ms);
 
+/* ckd_knn without any device allocation.  No counterpart in the reference: it
+ * serves callers that cannot allocate device memory while searching -- a host
+ * application that reserves all device memory up front and lets nothing reach
+ * the CUDA allocator later, or a latency-critical loop that cannot pay for the
+ * implicit synchronisation of an allocation.  Same arguments and exact result as
+ * ckd_knn; the search's scratch (query keys, processing order, a histogram of
+ * coarse leaf bins) lives in one fixed device array of about 18 MB that every
+ * device loading the library holds until exit.  Limits: nq <= 2097152 per call,
+ * k <= 64, tree depth < 92; larger requests fail with CKD_ERR_BAD_ARG.  All calls
+ * share the array, so calls that overlap on the GPU (other streams or threads)
+ * race and must be serialised by the caller.  The first call on a device looks
+ * up the array's address (cudaGetSymbolAddress); make it before any stream
+ * capture. */
+ckd_status ckd_knn_noalloc(const ckd_tree* tree, const double* q_dev, int64_t nq, int k,
+                           int sorted, double* dist_dev, int64_t* idx_dev, void* stream);
+
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);
