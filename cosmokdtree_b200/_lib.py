@@ -92,7 +92,21 @@ SIGNATURES = {
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],
     "ckd_box_fill": [_vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_exclusive_scan": [_vp, _vp, _i64, _vp],
+    "ckd_mlp_create": [ctypes.c_uint64, ctypes.POINTER(_vp)],
+    "ckd_mlp_free": [_vp],
+    "ckd_mlp_get": [_vp, _vp, _vp, _vp, _vp],
+    "ckd_mlp_set": [_vp, _vp, _vp, ctypes.c_float],
+    "ckd_mlp_features": [_vp, _vp, _i64, _int, _vp, _vp],
+    "ckd_mlp_grad": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],
+    "ckd_mlp_train": [_vp, _vp, _vp, _i64, _int, _int, ctypes.c_float, _vp, _vp],
+    "ckd_mlp_predict": [_vp, _vp, _i64, _vp, _vp],
+    "ckd_knn_learned": [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp, _vp],
 }
+
+MLP_FEATURES = 12
+MLP_HIDDEN = 64
+MLP_PARAMS = 5057
+MLP_NORM = 26
 _RESTYPES = {"ckd_last_error": ctypes.c_char_p, "ckd_launch_count": ctypes.c_int64}
 
 

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "ckd_common.cuh"
+#include "ckd_mlp.cuh"
 
 namespace ckd {
 
@@ -34,6 +35,9 @@ int knn_variant() { return g_knn_variant.load(std::memory_order_relaxed); }
 static std::atomic<int> g_knn_bps{0}, g_knn_wpb{4};
 int knn_blocks_per_sm() { return g_knn_bps.load(std::memory_order_relaxed); }
 int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
+static std::atomic<int> g_learned_kernel{0}, g_gather_wpb{2};
+int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); }
+int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
 void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -104,6 +108,8 @@ ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32
 ckd_status knn_stats(int enable, int64_t* out);
 ckd_status knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                        double* dist, int64_t* idx, cudaStream_t s);
+ckd_status knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, int64_t* nfb, cudaStream_t s);
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s);
@@ -343,6 +349,14 @@ ckd_status ckd_set_tuning(int key, int value) {
       if (value < 10 || value > 1000) return fail(CKD_ERR_BAD_ARG, "bucket radius factor must be 10..1000");
       set_knn_bucket_alpha(value / 100.0f);
       return CKD_OK;
+    case 4:
+      if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0 or 1");
+      g_learned_kernel.store(value);
+      return CKD_OK;
+    case 5:
+      if (value < 1 || value > 4) return fail(CKD_ERR_BAD_ARG, "gather warps per block must be 1..4");
+      g_gather_wpb.store(value);
+      return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
 }
@@ -355,6 +369,20 @@ ckd_status ckd_knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k
   if (nq == 0) return CKD_OK;
   if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
   return knn_noalloc(t, q, nq, k, sorted, dist, idx, (cudaStream_t)stream);
+}
+
+ckd_status ckd_knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq,
+                           int k, int sorted, double* dist, int64_t* idx, int64_t* n_fallback,
+                           void* stream) {
+  CKD_TRY(check_tree(t));
+  CKD_TRY(mlp_check(net));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (n_fallback) *n_fallback = 0;
+  if (nq == 0) return CKD_OK;
+  if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
+  if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
+  return knn_learned(t, net, q, nq, k, sorted, dist, idx, n_fallback, (cudaStream_t)stream);
 }
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,

@@ -41,6 +41,10 @@ int knn_variant();
 // tuning knobs (see ckd_set_tuning): blocks-per-SM cap (0 = none), warps per block
 int knn_blocks_per_sm();
 int knn_warps_per_block();
+// learned-bound search kernel: 0 bounded per-lane (k_knn_lane), 1 warp gather;
+// warps per block of the gather kernel
+int learned_kernel();
+int gather_warps_per_block();
 
 // events bracketing the main search kernel when kernel timing is on
 void timing_begin(cudaStream_t s);

@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include "ckd_common.cuh"
+#include "ckd_mlp.cuh"
 #include "ckd_scan.cuh"
 #include "ckd_traverse.cuh"
 
@@ -547,14 +548,25 @@ __global__ void __launch_bounds__(128) k_knn_screen(TreeView tv, const double* _
 // Lanes descend until they reach a leaf, then scan leaves together
 // (while-while structure), with the same FP32 screen, FP64 recheck and heap as
 // k_knn_screen.
-constexpr int kLaneStack = 64;
+//
+// BOUNDED: every query starts with its heap full of k sentinels (key r2[q],
+// id INT32_MAX) instead of HUGE, so pruning starts at the root.  A point is
+// accepted iff (d2, id) < the current worst, so every point with d2 <= r2[q] is
+// still seen; when no sentinel is left the heap holds the exact k nearest.  A
+// query that ends with a sentinel (fewer than k points within the bound) is
+// appended to miss[] for the unbounded rerun and its output row is not written.
+constexpr int kLaneStack = 128;
 
-template <int D, bool PER>
+template <int D, bool PER, bool BOUNDED = false>
 __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __restrict__ Q,
                                                   const int32_t* __restrict__ order, int64_t nq,
                                                   int k, int sorted, double* __restrict__ dist,
                                                   int64_t* __restrict__ idx,
-                                                  unsigned long long* __restrict__ stats) {
+                                                  unsigned long long* __restrict__ stats,
+                                                  const double* __restrict__ r2 = nullptr,
+                                                  int32_t* __restrict__ miss = nullptr,
+                                                  unsigned* __restrict__ nmiss = nullptr,
+                                                  const int32_t* __restrict__ qleaf = nullptr) {
   constexpr int NV = (D + 3) / 4;
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -579,18 +591,50 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
   unsigned long long* hk = keys + lane * KS;
   int32_t* hi = ids + lane * KS;
   const unsigned long long kHugeKey = (unsigned long long)__double_as_longlong(CKD_HUGE);
-  for (int s = 1; s <= k; ++s) {
-    hk[s] = kHugeKey;
-    hi[s] = -1;
-  }
-  unsigned long long wkey = kHugeKey;
-  int32_t wid = -1;
+  unsigned long long skey = kHugeKey;
+  int32_t sid = -1;
   float wd32 = FLT_MAX;
+  if (BOUNDED && valid) {
+    const double rr = r2[qi];
+    if (rr < CKD_HUGE) {
+      skey = (unsigned long long)__double_as_longlong(rr);
+      sid = 0x7fffffff;
+      wd32 = __double2float_ru(rr);
+    }
+  }
+  for (int s = 1; s <= k; ++s) {
+    hk[s] = skey;
+    hi[s] = sid;
+  }
+  unsigned long long wkey = skey;
+  int32_t wid = sid;
 
   int32_t sn[kLaneStack];
   float sd[kLaneStack];
   int top = 0;
   int32_t node = valid ? 0 : -1;
+  if (BOUNDED && valid && qleaf && sid == 0x7fffffff) {
+    // Start at the lowest ancestor of the query's leaf whose cell strictly
+    // contains the cube [q - r, q + r]^D: every point within the bound lies
+    // strictly inside that cell, hence in its subtree (and, periodic, is its own
+    // minimum image).  Inward-rounded FP32 cells and outward-rounded tests keep
+    // this conservative.
+    const float r32 = __fsqrt_ru(wd32);
+    int32_t a = qleaf[qi];
+    while (a > 0) {
+      const float* c = tv.cell32 + (int64_t)a * 2 * D;
+      bool inside = true;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        const float2 lh = __ldg(reinterpret_cast<const float2*>(c) + j);
+        inside = inside && __fsub_rd(__fsub_rd(qs.q32[j], r32), qs.dlt[j]) > lh.x &&
+                 __fadd_ru(__fadd_ru(qs.q32[j], r32), qs.dlt[j]) < lh.y;
+      }
+      if (inside) break;
+      a = load_meta(tv.meta, a).parent;
+    }
+    node = a < 0 ? 0 : a;
+  }
   while (node >= 0) {
     // ---- descend to a leaf, nearer child first
     NodeMeta m = load_meta(tv.meta, node);
@@ -727,7 +771,18 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
       if (lane == 0) atomicAdd(&stats[c], v);
     }
   }
-  if (sorted && valid) {
+  const bool missed = BOUNDED && valid && wid == 0x7fffffff;
+  unsigned missmask = 0;
+  if (BOUNDED) {
+    missmask = __ballot_sync(0xffffffffu, missed);
+    if (missmask) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(nmiss, (unsigned)__popc(missmask));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (missed) miss[base + __popc(missmask & ((1u << lane) - 1u))] = (int32_t)qi;
+    }
+  }
+  if (sorted && valid && !missed) {
     for (int end = k; end > 1; --end) {
       unsigned long long key = hk[end];
       int32_t id = hi[end];
@@ -762,6 +817,7 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
   for (int qq = 0; qq < 32; ++qq) {
     int64_t s2 = gw * 32 + qq;
     if (s2 >= nq) break;
+    if (BOUNDED && ((missmask >> qq) & 1u)) continue;
     int64_t row = order ? (int64_t)order[s2] : s2;
     const unsigned long long* rk = keys + qq * KS + 1;
     const int32_t* ri = ids + qq * KS + 1;
@@ -1696,6 +1752,326 @@ __global__ void __launch_bounds__(128) k_knn_bucket(TreeView tv, const double* _
   }
 }
 
+// ======================================= learned-radius gather search (bounded)
+// One warp serves 32 consecutive queries of the leaf order (spatially adjacent),
+// each with a predicted squared radius r2[q] from k_mlp_radius:
+//  1. gather: a warp-parallel frontier walk from the root collects every leaf
+//     whose FP32 box lies within R = max over lanes of sqrt(r2) of the bucket's
+//     bounding box;
+//  2. scan: for each gathered leaf that some lane's current bound reaches, the
+//     32 lanes screen the leaf's points together (the same leaf-relative FP32
+//     copy read by all lanes, one query per lane); a point whose FP32 lower bound
+//     is within the lane's bound joins the lane's candidate buffer;
+//  3. flush: when a buffer could overflow, and at the end, every lane evaluates
+//     its buffered candidates in FP64 (reference arithmetic) and inserts them into
+//     its heap, which starts full of (r2, INT32_MAX) sentinels as in the bounded
+//     per-lane kernel, so the bound only shrinks.
+// The screen loop is one instruction stream for all lanes; only the flushes
+// diverge.  A query ends exact when no sentinel remains.  Otherwise (fewer than k
+// points within its radius), or when the bucket's gather overflows, or when its
+// radius is not finite, the query is appended to miss[] for the plain rerun.
+constexpr int kGatherC = 48;         // candidate buffer per lane (>= 32)
+constexpr int kGatherLeaves = 384;   // gathered leaves per bucket
+constexpr int kGatherFront = 512;    // frontier capacity per level (two buffers)
+static_assert(2 * kGatherFront <= kGatherC * 32, "frontier shares the candidate buffer");
+
+__host__ __device__ inline size_t gather_smem_per_warp(int k) {
+  return (size_t)32 * heap_stride(k) * (sizeof(unsigned long long) + sizeof(int32_t)) +
+         (size_t)kGatherC * 32 * sizeof(int32_t) + (size_t)kGatherLeaves * sizeof(int32_t);
+}
+
+// replace the root of a 1-based max-heap (keys = FP64 bit patterns, ties by id)
+// by (key, id) and sift it down
+__device__ __forceinline__ void heap_replace_top(unsigned long long* hk, int32_t* hi, int k,
+                                                 unsigned long long key, int32_t id) {
+  int s = 1;
+  for (;;) {
+    int l = 2 * s;
+    if (l > k) break;
+    unsigned long long kc;
+    int32_t ic;
+    int c;
+    if (l < k) {
+      ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(hk + l);
+      int2 ii = *reinterpret_cast<const int2*>(hi + l);
+      bool right = kk.x < kk.y || (kk.x == kk.y && ii.x < ii.y);
+      kc = right ? kk.y : kk.x;
+      ic = right ? ii.y : ii.x;
+      c = right ? l + 1 : l;
+    } else {
+      kc = hk[l];
+      ic = hi[l];
+      c = l;
+    }
+    if (!(key < kc || (key == kc && id < ic))) break;
+    hk[s] = kc;
+    hi[s] = ic;
+    s = c;
+  }
+  hk[s] = key;
+  hi[s] = id;
+}
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_knn_gather(TreeView tv, const double* __restrict__ Q,
+                                                    const int32_t* __restrict__ order, int64_t nq,
+                                                    int k, int sorted, const double* __restrict__ r2,
+                                                    double* __restrict__ dist,
+                                                    int64_t* __restrict__ idx,
+                                                    int32_t* __restrict__ miss,
+                                                    unsigned* __restrict__ nmiss,
+                                                    unsigned long long* __restrict__ stats) {
+  constexpr int NV = (D + 3) / 4;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int KS = heap_stride(k);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem) + (size_t)w * 32 * KS;
+  int32_t* i32 = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned long long*>(smem) +
+                                            (size_t)nw * 32 * KS);
+  int32_t* ids = i32 + (size_t)w * 32 * KS;
+  int32_t* cand = i32 + (size_t)nw * 32 * KS + (size_t)w * kGatherC * 32;  // [slot][lane]
+  int32_t* front = cand;  // gather phase only
+  int32_t* leaves = i32 + (size_t)nw * 32 * KS + (size_t)nw * kGatherC * 32 +
+                    (size_t)w * kGatherLeaves;
+
+  const int64_t gw = (int64_t)blockIdx.x * nw + w;
+  const int64_t slot = gw * 32 + lane;
+  const bool valid = slot < nq;
+  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    q[j] = valid ? Q[qi * D + j] : 0.0;
+    qs.q32[j] = __double2float_rn(q[j]);
+    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+  }
+  // heap full of sentinels at the predicted radius
+  const double rr = valid ? r2[qi] : 0.0;
+  const bool part = valid && rr < CKD_HUGE;  // takes part in the bounded search
+  unsigned long long* hk = keys + lane * KS;
+  int32_t* hi = ids + lane * KS;
+  const unsigned long long skey =
+      part ? (unsigned long long)__double_as_longlong(rr) : 0ull;
+  for (int s = 1; s <= k; ++s) {
+    hk[s] = skey;
+    hi[s] = 0x7fffffff;
+  }
+  unsigned long long wkey = skey;
+  int32_t wid = 0x7fffffff;
+  float wd32 = part ? __double2float_ru(rr) : -1.0f;  // -1: never passes a screen
+
+  // ---- bucket box and gather radius over the participating lanes
+  float blo[D], bhi[D], dlt[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float lo = part ? __double2float_rd(q[j]) : FLT_MAX;
+    float hh = part ? __double2float_ru(q[j]) : -FLT_MAX;
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(FULL, lo, o));
+      hh = fmaxf(hh, __shfl_xor_sync(FULL, hh, o));
+    }
+    blo[j] = lo;
+    bhi[j] = hh;
+    dlt[j] = kTwoM21 * (fmaxf(fabsf(lo), fabsf(hh)) + tv.slack[j]) * 1.0001f;
+  }
+  float R = part ? __fsqrt_ru(wd32) : 0.0f;
+  for (int o = 16; o > 0; o >>= 1) R = fmaxf(R, __shfl_xor_sync(FULL, R, o));
+  const float R2 = __fmul_ru(R, R);
+  const bool any_part = __any_sync(FULL, part);
+
+  // ---- 1. gather the leaves within R of the bucket box
+  int nlv = 0;
+  bool overflow = false;
+  if (any_part) {
+    int nf = 1, cur = 0;
+    if (lane == 0) front[0] = 0;
+    __syncwarp();
+    while (nf > 0 && !overflow) {
+      int nn = 0;
+      for (int base = 0; base < nf; base += 32) {
+        const int fi = base + lane;
+        const int32_t node = fi < nf ? front[cur * kGatherFront + fi] : -1;
+        bool need = false, leaf = false;
+        NodeMeta nm;
+        if (node >= 0) {
+          if (stats) st[0] += 1;
+          need = boxbox_gap_lb<D, PER>(tv, blo, bhi, tv.box32 + (int64_t)node * 2 * D, dlt) <= R2;
+          nm = load_meta(tv.meta, node);
+          leaf = nm.left < 0;
+        }
+        const unsigned im = __ballot_sync(FULL, need && !leaf);
+        const int ipos = nn + 2 * __popc(im & lt_mask);
+        if (need && !leaf && ipos + 1 < kGatherFront) {
+          front[(1 - cur) * kGatherFront + ipos] = nm.left;
+          front[(1 - cur) * kGatherFront + ipos + 1] = nm.left + 1;
+        }
+        nn += 2 * __popc(im);
+        const unsigned lm = __ballot_sync(FULL, need && leaf);
+        const int lpos = nlv + __popc(lm & lt_mask);
+        if (need && leaf && lpos < kGatherLeaves) leaves[lpos] = node;
+        nlv += __popc(lm);
+      }
+      if (nn > kGatherFront || nlv > kGatherLeaves) overflow = true;
+      __syncwarp();
+      nf = nn;
+      cur = 1 - cur;
+    }
+  }
+  if (stats && lane == 0) st[1] += nlv;
+
+  // ---- 2./3. screen the gathered leaves, flushing candidates into the heaps
+  int cnt = 0;
+  auto flush = [&]() {
+    const int mx = __reduce_max_sync(FULL, (unsigned)cnt);
+    if (stats && lane == 0) st[4] += 1;
+    for (int j = 0; j < mx; ++j) {
+      if (j < cnt) {
+        if (stats) st[5] += 1;
+        const int32_t p = cand[j * 32 + lane];
+        const double d2 = point_d2<D, PER>(tv, q, p);
+        const unsigned long long key = (unsigned long long)__double_as_longlong(d2);
+        if (key <= wkey) {
+          const int32_t id = __ldg(&tv.ids[p]);
+          if (key < wkey || id < wid) {
+            if (stats) st[6] += 1;
+            heap_replace_top(hk, hi, k, key, id);
+            wkey = hk[1];
+            wid = hi[1];
+            wd32 = __double2float_ru(__longlong_as_double((long long)wkey));
+          }
+        }
+      }
+    }
+    cnt = 0;
+    __syncwarp();
+  };
+  if (!overflow) {
+    __syncwarp();  // the frontier shared the candidate buffer
+    for (int li = 0; li < nlv; ++li) {
+      const int32_t leaf = leaves[li];
+      const bool reach = part && node_mind_lb<D, PER>(tv, qs, leaf) <= wd32;
+      if (!__any_sync(FULL, reach)) continue;
+      if (stats) st[2] += reach;
+      const NodeMeta m = load_meta(tv.meta, leaf);
+      float qr[D], e[D];
+      {
+        const double* b = tv.box + (int64_t)leaf * 2 * D;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          double lo = __ldg(&b[2 * j]), hh = __ldg(&b[2 * j + 1]);
+          double c = leaf_centre(lo, hh);
+          double r = fmax(c - lo, hh - c);
+          double x = q[j] - c;
+          if (PER) {
+            double h = 0.5 * tv.L[j];
+            if (x > h) x -= tv.L[j];
+            else if (x < -h) x += tv.L[j];
+          }
+          qr[j] = __double2float_rn(x);
+          e[j] = kTwoM21 * (float)(r + fabs(x) + (PER ? tv.L[j] : 0.0)) * 1.0001f + 1e-37f;
+        }
+      }
+      for (int base = 0; base < m.count; base += 32) {
+        const int c = min(32, m.count - base);
+        if (__any_sync(FULL, cnt + c > kGatherC)) flush();
+        const int32_t p0 = m.start + base;
+        if (stats) st[3] += c;
+        for (int i = 0; i < c; ++i) {
+          float v[4 * NV];
+#pragma unroll
+          for (int h = 0; h < NV; ++h) {
+            float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+            v[4 * h] = f.x;
+            v[4 * h + 1] = f.y;
+            v[4 * h + 2] = f.z;
+            v[4 * h + 3] = f.w;
+          }
+          float s = 0.0f;
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            float a = fabsf(v[j] - qr[j]);
+            if (PER) a = fminf(a, (float)tv.L[j] - a);
+            a = fmaxf(a - e[j], 0.0f);
+            s = fmaf(a, a, s);
+          }
+          if (s * kShrink <= wd32) {
+            cand[cnt * 32 + lane] = p0 + i;
+            ++cnt;
+          }
+        }
+      }
+    }
+    flush();
+  }
+
+  // ---- queries left with a sentinel go to the plain rerun
+  const bool missed = valid && (!part || overflow || wid == 0x7fffffff);
+  const unsigned missmask = __ballot_sync(FULL, missed);
+  if (missmask) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(nmiss, (unsigned)__popc(missmask));
+    base = __shfl_sync(FULL, base, 0);
+    if (missed) miss[base + __popc(missmask & lt_mask)] = (int32_t)qi;
+    if (stats && lane == 0) st[7] += __popc(missmask);
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = st[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+  if (sorted && valid && !missed) {
+    for (int end = k; end > 1; --end) {
+      unsigned long long key = hk[end];
+      int32_t id = hi[end];
+      hk[end] = hk[1];
+      hi[end] = hi[1];
+      int s = 1;
+      for (;;) {
+        int l = 2 * s;
+        if (l >= end) break;
+        int c = l;
+        unsigned long long kc = hk[l];
+        int32_t ic = hi[l];
+        if (l + 1 < end) {
+          unsigned long long kr = hk[l + 1];
+          int32_t ir = hi[l + 1];
+          if (kc < kr || (kc == kr && ic < ir)) {
+            c = l + 1;
+            kc = kr;
+            ic = ir;
+          }
+        }
+        if (!(key < kc || (key == kc && id < ic))) break;
+        hk[s] = kc;
+        hi[s] = ic;
+        s = c;
+      }
+      hk[s] = key;
+      hi[s] = id;
+    }
+  }
+  __syncwarp();
+  for (int qq = 0; qq < 32; ++qq) {
+    const int64_t s2 = gw * 32 + qq;
+    if (s2 >= nq) break;
+    if ((missmask >> qq) & 1u) continue;
+    const int64_t row = order ? (int64_t)order[s2] : s2;
+    const unsigned long long* rk = keys + qq * KS + 1;
+    const int32_t* ri = ids + qq * KS + 1;
+    for (int j = lane; j < k; j += 32) {
+      dist[row * k + j] = sqrt(__longlong_as_double((long long)rk[j]));
+      idx[row * k + j] = (int64_t)ri[j];
+    }
+  }
+}
+
 // bucket list: for every leaf holding queries, ceil(count / 32) buckets
 __global__ void k_bucket_count(const NodeMeta* __restrict__ meta, int32_t n_nodes,
                                const int32_t* __restrict__ off, int32_t* __restrict__ nb) {
@@ -2015,6 +2391,95 @@ ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int so
   if (order) dev_free(order, s);
   if (qleaf) dev_free(qleaf, s);
   return st;
+}
+
+// ===================================================================
+// kNN with the learned bound (ckd_knn_learned)
+//
+// locate + order the queries, predict each query's squared k-th distance
+// (k_mlp_radius), run the bounded per-lane search, then rerun the queries it
+// could not settle with the plain search.  The bounded kernel needs the FP32
+// screen, k <= kSmemK and a stack deep enough for the tree; otherwise every query
+// takes the plain path.
+namespace {
+
+template <int D, bool PER>
+ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq,
+                            int k, int sorted, double* dist, int64_t* idx, int64_t* nfb_out,
+                            cudaStream_t s) {
+  int32_t *order = nullptr, *qleaf = nullptr, *miss = nullptr;
+  double* r2 = nullptr;
+  unsigned* nmiss = nullptr;
+  CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
+  CKD_CUDA(dev_alloc((void**)&qleaf, sizeof(int32_t) * nq, s));
+  CKD_CUDA(dev_alloc((void**)&r2, sizeof(double) * nq, s));
+  CKD_CUDA(dev_alloc((void**)&miss, sizeof(int32_t) * nq, s));
+  CKD_CUDA(dev_alloc((void**)&nmiss, sizeof(unsigned), s));
+  CKD_CUDA(cudaMemsetAsync(nmiss, 0, sizeof(unsigned), s));
+  ckd_status st = order_impl<D>(t, q, nq, order, qleaf, s);
+  if (st == CKD_OK) {
+    timing_begin(s);
+    st = mlp_radius(t, net, q, order, qleaf, nq, k, r2, s);
+  }
+  if (st == CKD_OK && learned_kernel() == 0) {
+    const int nw = knn_warps_per_block();
+    const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    const int bps = knn_blocks_per_sm();
+    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
+    cudaError_t e = cudaFuncSetAttribute(k_knn_lane<D, PER, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane)");
+    k_knn_lane<D, PER, true><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist,
+                                                         idx, knn_stats_buffer(), r2, miss, nmiss,
+                                                         qleaf);
+    note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) st = cuda_fail(e, "k_knn_lane (bounded)");
+  } else if (st == CKD_OK) {
+    const int nw = gather_warps_per_block();
+    const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+    const size_t sm = (size_t)nw * gather_smem_per_warp(k);
+    cudaError_t e = cudaFuncSetAttribute(k_knn_gather<D, PER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_knn_gather)");
+    k_knn_gather<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, r2, dist,
+                                                     idx, miss, nmiss, knn_stats_buffer());
+    note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) st = cuda_fail(e, "k_knn_gather");
+  }
+  unsigned nm = 0;
+  if (st == CKD_OK) {
+    cudaError_t e = cudaMemcpyAsync(&nm, nmiss, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "reading the fallback count");
+    else if ((int64_t)nm > nq) st = fail(CKD_ERR_CUDA, "internal error: fallback list overflow");
+  }
+  if (st == CKD_OK && nm > 0)
+    st = knn_launch<D, PER>(t, q, miss, nullptr, (int64_t)nm, k, sorted, dist, idx, s, 3);
+  if (st == CKD_OK) timing_end(s);
+  if (nfb_out) *nfb_out = nm;
+  for (void* p : {(void*)order, (void*)qleaf, (void*)r2, (void*)miss, (void*)nmiss}) dev_free(p, s);
+  return st;
+}
+
+}  // namespace
+
+ckd_status knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, int64_t* nfb, cudaStream_t s) {
+  if (!(t->screen_ok && t->depth < kLaneStack - 1 && k <= kSmemK)) {
+    if (nfb) *nfb = nq;
+    return knn_run(t, q, nq, k, sorted, dist, idx, s);
+  }
+  switch (t->d * 2 + (t->periodic ? 1 : 0)) {
+#define CKD_LB(DD)                                                                          \
+  case 2 * DD: return knn_learned_impl<DD, false>(t, net, q, nq, k, sorted, dist, idx, nfb, s); \
+  case 2 * DD + 1: return knn_learned_impl<DD, true>(t, net, q, nq, k, sorted, dist, idx, nfb, s);
+    CKD_LB(1) CKD_LB(2) CKD_LB(3) CKD_LB(4) CKD_LB(5) CKD_LB(6) CKD_LB(7) CKD_LB(8)
+#undef CKD_LB
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
 }
 
 // ===================================================================

@@ -97,9 +97,11 @@ ckd_status ckd_knn_ordered(const ckd_tree* tree, const double* q_dev, int64_t nq
 int64_t ckd_launch_count(void);
 
 /* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (the
- * FP32-screened kernel when k <= 64 and coordinates allow it), 1 = FP64-only
- * traversal, 2 = FP32-screened whenever possible.  Every variant returns the same
- * exact result. */
+ * per-lane FP32-screened traversal when k <= 64, the coordinates allow the FP32
+ * screen and the tree is shallow enough, else 2), 1 = FP64-only packet
+ * traversal, 2 = FP32-screened packet traversal, 3 = per-lane traversal,
+ * 4 = bottom-up per-lane search, 5 = persistent per-lane search, 6 = warp per
+ * bucket with a density radius.  Every variant returns the same exact result. */
 ckd_status ckd_set_knn_variant(int variant);
 
 /* Process-wide launch tuning of the search kernels (no reference counterpart;
@@ -107,7 +109,9 @@ ckd_status ckd_set_knn_variant(int variant);
  * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
  * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
  * of the kNN kernel (1..8, default 4); key 3: radius factor of the warp-per-bucket
- * kNN search in hundredths (default 150 = 1.5x the density estimate). */
+ * kNN search in hundredths (default 150 = 1.5x the density estimate); key 4:
+ * search kernel of ckd_knn_learned (0 = bounded per-lane traversal, default;
+ * 1 = warp gather); key 5: warps per block of the warp-gather kernel (1..4, default 2). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference
@@ -168,6 +172,62 @@ ckd_status ckd_box_fill(const ckd_tree* tree, const double* boxes_dev, int64_t n
 
 /* out_dev[0] = 0, out_dev[i+1] = in_dev[0] + ... + in_dev[i]  (n+1 outputs). */
 ckd_status ckd_exclusive_scan(const int64_t* in_dev, int64_t* out_dev, int64_t n, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Learned k-th-neighbour distance bound (no counterpart in the reference; it
+ * speeds up ckd_knn without changing its results).
+ *
+ * A 12 -> 64 -> 64 -> 1 ReLU network (BF16 weights, FP32 arithmetic) predicts
+ * y = log2(distance to the k-th neighbour) of a query from features of its leaf
+ * and ancestors (ckd_mlp_features).  ckd_knn_learned seeds each query's heap with
+ * the bound r = 2^(y + margin): the traversal prunes from the root, and every
+ * query with fewer than k points within r is searched again without a bound, so
+ * the result is exactly ckd_knn's.  The parameter vector is FP32, layout
+ * W1[64][12], b1[64], W2[64][64], b2[64], W3[64], b3 (CKD_MLP_PARAMS floats);
+ * the normalisation vector holds the feature means[12], 1/sigma[12], and the
+ * target mean and sigma (CKD_MLP_NORM floats). */
+#define CKD_MLP_FEATURES 12
+#define CKD_MLP_HIDDEN 64
+#define CKD_MLP_PARAMS 5057
+#define CKD_MLP_NORM 26
+typedef struct ckd_mlp ckd_mlp;
+
+/* New network on the current device, weights initialised from `seed`. */
+ckd_status ckd_mlp_create(uint64_t seed, ckd_mlp** out);
+ckd_status ckd_mlp_free(ckd_mlp* net);
+/* Host copies of the FP32 weights / normalisation / margin / Adam step count;
+ * any output may be NULL.  Synchronous. */
+ckd_status ckd_mlp_get(const ckd_mlp* net, float* params_host, float* norm_host, float* margin,
+                       int64_t* steps);
+/* Replace weights (resets Adam) and/or normalisation (either may be NULL) and set
+ * the margin (log2 units added to every prediction).  Synchronous. */
+ckd_status ckd_mlp_set(ckd_mlp* net, const float* params_host, const float* norm_host,
+                       float margin);
+/* feat_dev[nq][12] = features of each query for neighbour count k. */
+ckd_status ckd_mlp_features(const ckd_tree* tree, const double* q_dev, int64_t nq, int k,
+                            float* feat_dev, void* stream);
+/* Gradient (grad_host[CKD_MLP_PARAMS]) and value (*loss) of the mean squared error
+ * (1/n) sum (z - (t - t_mean) / t_sigma)^2 of the normalised output z over n
+ * samples, at the current BF16 weights.  The first use of an untrained network
+ * sets the normalisation from these samples.  Synchronous. */
+ckd_status ckd_mlp_grad(ckd_mlp* net, const float* feat_dev, const float* target_dev, int64_t n,
+                        float* grad_host, float* loss, void* stream);
+/* `epochs` passes of Adam (lr, betas 0.9/0.999, eps 1e-8) over the samples in the
+ * given order, `batch` samples per step; loss_host[e] (may be NULL) receives the
+ * mean loss of epoch e.  Targets are log2 of exact k-th-neighbour distances.
+ * Synchronous. */
+ckd_status ckd_mlp_train(ckd_mlp* net, const float* feat_dev, const float* target_dev, int64_t n,
+                         int batch, int epochs, float lr, float* loss_host, void* stream);
+/* y_dev[n] = predicted log2 k-th distance (margin not added). */
+ckd_status ckd_mlp_predict(const ckd_mlp* net, const float* feat_dev, int64_t n, float* y_dev,
+                           void* stream);
+/* ckd_knn with the learned bound.  Same results as ckd_knn; *n_fallback (may be
+ * NULL) receives the number of queries that needed the unbounded rerun (all of
+ * them when the bounded kernel does not apply: k > 64 or a very deep tree).
+ * Synchronises `stream` once to read that count. */
+ckd_status ckd_knn_learned(const ckd_tree* tree, const ckd_mlp* net, const double* q_dev,
+                           int64_t nq, int k, int sorted, double* dist_dev, int64_t* idx_dev,
+                           int64_t* n_fallback, void* stream);
 
 #ifdef __cplusplus
 }
