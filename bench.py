@@ -1,11 +1,14 @@
 #!/usr/bin/env python
 """Benchmark: exact kNN queries/s (k=32, self-query) over a 16.7M-point clustered
-periodic catalogue on one B200, plus build Mpt/s.
+periodic catalogue on one B200 -- learned-bound search (headline ``value``) and the
+plain search (``plain``), both exact and checked equal -- plus build Mpt/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 A step is one kNN pass of every point of the catalogue (2^24 queries, k=32,
-sorted) through the library with inputs resident in HBM.  Timing: CUDA events on
+sorted) through the library with inputs resident in HBM.  The network is trained
+beforehand (untimed, like the tree build) on 10^6 exact k-th distances of a
+separate catalogue drawn with another seed.  Timing: CUDA events on
 the launching stream, barrier + synchronize around the timed region, max over
 ranks.  Inputs (tree ~0.6 GB, outputs 8.6 GB per step) are far larger than L2.
 Under torchrun each rank builds and searches its own catalogue (seed + rank) with
@@ -257,89 +260,125 @@ def main():
     Q = Pd
     dist_t = torch.empty((nq, k), dtype=torch.float64, device="cuda")
     idx_t = torch.empty((nq, k), dtype=torch.int64, device="cuda")
-    order = torch.empty(nq, dtype=torch.int32, device="cuda")
+    dist_l = torch.empty((nq, k), dtype=torch.float64, device="cuda")
+    idx_l = torch.empty((nq, k), dtype=torch.int64, device="cuda")
+    qp, dp, ip = (ctypes.c_void_p(x.data_ptr()) for x in (Q, dist_t, idx_t))
+    dlp, ilp = (ctypes.c_void_p(x.data_ptr()) for x in (dist_l, idx_l))
+    nfb = ctypes.c_int64()
 
-    def step(ev=None):
-        if ev is not None:
-            ev[0].record(stream)
-        _lib.check(L.ckd_knn(tree.handle, ctypes.c_void_p(Q.data_ptr()), nq, k, 1,
-                             ctypes.c_void_p(dist_t.data_ptr()),
-                             ctypes.c_void_p(idx_t.data_ptr()), sp))
-        if ev is not None:
-            ev[1].record(stream)
+    def plain_step():
+        _lib.check(L.ckd_knn(tree.handle, qp, nq, k, 1, dp, ip, sp))
 
-    def kernel_ms(reps=3):
-        """Average device time of the main search kernel alone (CUDA events
-        recorded by the library around that launch)."""
+    def learned_step():
+        _lib.check(L.ckd_knn_learned(tree.handle, lb.handle, qp, nq, k, 1, dlp, ilp,
+                                     ctypes.byref(nfb), sp))
+
+    def timed(fn, steps, warmup):
+        """W untimed steps, then K steps between barrier + synchronize; max over ranks."""
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+        l0 = L.ckd_launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for s_ in range(steps):
+            evs[s_][0].record(stream)
+            fn()
+            evs[s_][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        total = allmax(t0.elapsed_time(t1))
+        return total, [e[0].elapsed_time(e[1]) for e in evs], L.ckd_launch_count() - l0
+
+    def kernel_ms(fn, reps=3):
+        """Device time of the search kernels alone (CUDA events the library records
+        on the launching stream around them)."""
         _lib.check(L.ckd_set_kernel_timing(1))
         vals = []
         for _ in range(reps):
-            step()
+            fn()
             v = ctypes.c_float()
             _lib.check(L.ckd_kernel_ms(ctypes.byref(v)))
             vals.append(v.value)
         _lib.check(L.ckd_set_kernel_timing(0))
         return float(np.mean(vals))
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
-    if args.stats:
+    def stats_of(fn):
+        st = (ctypes.c_int64 * 8)()
         _lib.check(L.ckd_knn_stats(1, None))
-    launches0 = L.ckd_launch_count()
+        fn()
+        _lib.check(L.ckd_knn_stats(0, st))
+        return [v / nq for v in st]
+
+    # ---- learned bound: trained on a separate catalogue (seed + 2), 10^6 samples
+    from cosmokdtree_b200.learned import LearnedBound
+    t_tr = time.perf_counter()
+    P_tr = make_points(name, seed_offset=rank + 2)
+    tree_tr = kdtree.build_kdtree(torch.from_numpy(P_tr).cuda(), leaf=leaf, boxsize=box)
+    rng_tr = np.random.default_rng(3 + rank)
+    n_train = min(1_000_000, P_tr.shape[0])
+    Q_tr = torch.from_numpy(P_tr[rng_tr.integers(0, P_tr.shape[0], n_train)]).cuda()
+    lb = LearnedBound(seed=rank)
+    fit = lb.fit(tree_tr, Q_tr, k, epochs=30 if not args.profile else 4, batch=4096, lr=3e-3,
+                 quantile=0.97)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t_tr
+    tree_tr.close()
+    del Q_tr
+
+    # ---- plain search
     with ClockSampler(local) as clk:
-        barrier()
-        torch.cuda.synchronize()
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_start.record(stream)
-        for s in range(args.steps):
-            step(evs[s])
-        t_end.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    launches = L.ckd_launch_count() - launches0
-    total_ms = allmax(t_start.elapsed_time(t_end))
-    step_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    knn_kernel_ms = kernel_ms()
-    ms_per_step = total_ms / args.steps
-    value = world * nq * args.steps / (total_ms / 1e3)
+        plain_total, plain_steps, plain_launches = timed(plain_step, args.steps, args.warmup)
+        learned_total, learned_steps, launches = timed(learned_step, args.steps, args.warmup)
+    fallback = int(nfb.value)
+    plain_kernel_ms = kernel_ms(plain_step)
+    learned_kernel_ms = kernel_ms(learned_step)
+    exact = bool(torch.equal(idx_l, idx_t) and torch.equal(dist_l, dist_t))
+    exact = allmax(0.0 if exact else 1.0) == 0.0
+    plain_value = world * nq * args.steps / (plain_total / 1e3)
+    value = world * nq * args.steps / (learned_total / 1e3)
+    ms_per_step = learned_total / args.steps
     clocks = clk.summary()
     stats = None
     if args.stats:
-        st = (ctypes.c_int64 * 8)()
-        _lib.check(L.ckd_knn_stats(0, st))
-        names = ["pops", "needed_pops", "leaf_visits", "points_screened", "insert_rounds",
-                 "fp64_evals", "inserts", "lanes_on_leaf_visits"]
-        warps = args.steps * ((nq + 31) // 32)
-        stats = {nm: st[i] / warps for i, nm in enumerate(names)}
-        stats["per_query_fp64_evals"] = st[5] / (args.steps * nq)
-        stats["per_query_inserts"] = st[6] / (args.steps * nq)
+        names = ["node_tests", "gathered_leaves", "leaf_scans", "points_screened", "flushes",
+                 "fp64_evals", "heap_inserts", "misses"]
+        stats = {"plain_per_query": dict(zip(names, stats_of(plain_step))),
+                 "learned_per_query": dict(zip(names, stats_of(learned_step)))}
     if args.profile:
         if rank == 0:
-            print(json.dumps({"profile": True, "workload": name, "ms_per_step": ms_per_step,
-                              "variant": args.variant, "tune": args.tune, "stats_per_warp": stats,
-                              "knn_kernel_ms": knn_kernel_ms, "step_ms": float(np.mean(step_ms)),
-                              "build_ms": build_ms_v, "depth": tree.depth, "n_nodes": tree.n_nodes}))
+            print(json.dumps({"profile": True, "workload": name, "variant": args.variant,
+                              "tune": args.tune, "plain_ms": plain_total / args.steps,
+                              "learned_ms": ms_per_step, "plain_kernel_ms": plain_kernel_ms,
+                              "learned_kernel_ms": learned_kernel_ms, "fallback": fallback,
+                              "exact": exact, "stats": stats, "build_ms": build_ms_v,
+                              "depth": tree.depth, "n_nodes": tree.n_nodes}))
         tree.close()
         return 0
 
-    # ---- end to end through the public API with host buffers
-    e2e_ms = []
-    for it in range(args.e2e_steps + 1):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        hd, hi = kdtree.knn_search(tree, P, k, sorted=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if it > 0:
-            e2e_ms.append(e0.elapsed_time(e1))
-    e2e_ms_v = allmax(float(np.mean(e2e_ms)))
+    # ---- end to end through the public API with host buffers (learned and plain)
+    def e2e(fn):
+        vals = []
+        for it in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it > 0:
+                vals.append(e0.elapsed_time(e1))
+        return allmax(float(np.mean(vals))), res
 
-    out = None
+    e2e_ms_v, (hd, hi) = e2e(lambda: lb.knn(tree, P, k, sorted=True))
+    e2e_plain_ms, _ = e2e(lambda: kdtree.knn_search(tree, P, k, sorted=True))
+
     if rank == 0:
         import oracle
         peak, peak_kind = measured_peaks()
@@ -354,8 +393,13 @@ def main():
         parity = bool(np.array_equal(oi, hi[samp]) and np.array_equal(od, hd[samp]))
         ab = otree.knn_algbytes(P[samp], k, od[:, -1] ** 2)
         bytes_per_q = ab["bytes"] / len(samp)
-        knn_avg_ms = knn_kernel_ms
-        achieved = bytes_per_q * nq / (knn_avg_ms / 1e3) / 1e9
+
+        def roof(ms, kernel):
+            a = bytes_per_q * nq / (ms / 1e3) / 1e9
+            return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+                    "traffic": None, "kernel": kernel, "kernel_ms": ms,
+                    "alg_bytes_per_query": bytes_per_q, "peak_kind": peak_kind}
+
         cpu = None
         if world == 1 and not args.no_cpu:
             rate, m, dt = cpu_knn_rate(otree, P, k, target_s=args.cpu_seconds)
@@ -368,24 +412,38 @@ def main():
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(name),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_knn_bucket", "kernel_ms": knn_avg_ms,
-                         "alg_bytes_per_query": bytes_per_q, "peak_kind": peak_kind},
+            "roofline": roof(learned_kernel_ms, "k_mlp_radius + k_knn_lane (bounded) + rerun"),
             "cpu_baseline": cpu,
             "e2e": {"value": world * nq / (e2e_ms_v / 1e3), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * 3 * 8, "d2h_bytes_per_step": nq * k * 16,
                     "ms_per_step": e2e_ms_v},
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "learned": {"method": "learned-bound kNN (MLP 12-64-64-1, BF16 weights)",
+                        "value": value, "speedup_vs_plain": value / plain_value,
+                        "exact_vs_plain": exact, "fallback_queries": fallback,
+                        "fallback_rate": fallback / nq, "kernel_ms": learned_kernel_ms,
+                        "train_s": train_s, "train_samples": fit["n_train"],
+                        "train_catalogue_seed_offset": 2, "margin_log2": fit["margin"],
+                        "holdout_rms_log2": fit["holdout_rms_log2"],
+                        "holdout_rerun_rate": fit["holdout_rerun_rate"],
+                        "final_loss": fit["loss"][-1]},
+            "plain": {"value": plain_value, "ms_per_step": plain_total / args.steps,
+                      "kernel_ms": plain_kernel_ms, "gpu_launches": int(plain_launches),
+                      "roofline": roof(plain_kernel_ms, "k_knn_lane"),
+                      "e2e_queries_per_s": world * nq / (e2e_plain_ms / 1e3)},
             "build": {"ms": build_ms_v, "mpts_per_s": n / (build_ms_v / 1e3) / 1e6,
                       "cpu_s": cpu_build_s, "cpu_mpts_per_s": n / cpu_build_s / 1e6,
                       "n_nodes": tree.n_nodes, "depth": tree.depth},
-            "breakdown_ms": {"step": float(np.mean(step_ms)), "knn_kernel": knn_avg_ms},
+            "breakdown_ms": {"learned_step": float(np.mean(learned_steps)),
+                             "plain_step": float(np.mean(plain_steps))},
             "parity_sample": {"rows": int(len(samp)), "bit_exact": parity},
         }
+        if stats:
+            out["stats"] = stats
         print(json.dumps(out))
     tree.close()
+    lb.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
