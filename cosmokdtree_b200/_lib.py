@@ -92,6 +92,12 @@ SIGNATURES = {
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],
     "ckd_box_fill": [_vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_exclusive_scan": [_vp, _vp, _i64, _vp],
+    "ckd_forest_build": [_vp, _pi64, _i64, _int, _int, _int, _pdbl, _int, _vp,
+                         ctypes.POINTER(_vp)],
+    "ckd_forest_info": [_vp, _pi64, _pi64],
+    "ckd_forest_knn": [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
+    "ckd_forest_box_count": [_vp, _vp, _vp, _i64, _vp, _vp],
+    "ckd_forest_box_fill": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_mlp_create": [ctypes.c_uint64, ctypes.POINTER(_vp)],
     "ckd_mlp_free": [_vp],
     "ckd_mlp_get": [_vp, _vp, _vp, _vp, _vp],

@@ -114,7 +114,10 @@ ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bo
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s);
 ckd_status box_run(const ckd_tree* t, const double* boxes, int64_t nb, bool fill, int64_t* counts,
-                   const int64_t* offsets, int64_t* idx, cudaStream_t s);
+                   const int64_t* offsets, int64_t* idx, cudaStream_t s,
+                   const int32_t* broot = nullptr);
+ckd_status forest_knn(const ckd_tree* t, const double* q, const int32_t* qroot, int64_t nq, int k,
+                      int sorted, double* dist, int64_t* idx, cudaStream_t s);
 
 static ckd_status check_device(int* dev_out) {
   int dev = 0;
@@ -159,8 +162,13 @@ int ckd_version(void) { return 100; }
 
 const char* ckd_last_error(void) { return g_err.c_str(); }
 
-ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf, const double* boxsize,
-                     int pts_on_device, void* stream, ckd_tree** out) {
+}  // extern "C"
+
+namespace ckd {
+// Shared by ckd_build and ckd_forest_build: off = tree offsets (n_trees + 1).
+static ckd_status build_common(const void* pts, int64_t n, int d, int dtype, int leaf,
+                               const double* boxsize, int pts_on_device, void* stream,
+                               std::vector<int64_t> off, ckd_tree** out) {
   if (!out) return fail(CKD_ERR_BAD_ARG, "null output handle pointer");
   *out = nullptr;
   if (!pts) return fail(CKD_ERR_BAD_ARG, "null points pointer");
@@ -175,6 +183,8 @@ ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf, con
   ckd_tree* t = new ckd_tree();
   t->device = dev;
   t->n = n;
+  t->n_trees = (int64_t)off.size() - 1;
+  t->tree_off = std::move(off);
   t->d = d;
   t->leaf = leaf;
   t->input_dtype = dtype;
@@ -211,6 +221,92 @@ ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf, con
   return CKD_OK;
 }
 
+static ckd_status check_single(const ckd_tree* t) {
+  CKD_TRY(check_tree(t));
+  if (t->n_trees != 1)
+    return fail(CKD_ERR_BAD_ARG, "the handle is a forest; use the ckd_forest_* entry points");
+  return CKD_OK;
+}
+
+static ckd_status check_forest(const ckd_tree* t) {
+  CKD_TRY(check_tree(t));
+  return CKD_OK;
+}
+}  // namespace ckd
+
+extern "C" {
+
+ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf, const double* boxsize,
+                     int pts_on_device, void* stream, ckd_tree** out) {
+  return build_common(pts, n, d, dtype, leaf, boxsize, pts_on_device, stream, {0, n}, out);
+}
+
+ckd_status ckd_forest_build(const void* pts, const int64_t* offsets, int64_t n_trees, int d,
+                            int dtype, int leaf, const double* boxsize, int pts_on_device,
+                            void* stream, ckd_tree** out) {
+  if (out) *out = nullptr;
+  if (!offsets || n_trees < 1) return fail(CKD_ERR_BAD_ARG, "a forest needs offsets of >= 1 trees");
+  if (n_trees >= 0x7fffffffll) return fail(CKD_ERR_BAD_ARG, "too many trees");
+  std::vector<int64_t> off(offsets, offsets + n_trees + 1);
+  if (off[0] != 0) return fail(CKD_ERR_BAD_ARG, "forest offsets must start at 0");
+  for (int64_t i = 0; i < n_trees; ++i)
+    if (off[i + 1] <= off[i]) return fail(CKD_ERR_BAD_ARG, "every tree needs at least one point");
+  const int64_t total = off[n_trees];  // before `off` is moved into the call
+  return build_common(pts, total, d, dtype, leaf, boxsize, pts_on_device, stream, std::move(off),
+                      out);
+}
+
+ckd_status ckd_forest_info(const ckd_tree* t, int64_t* n_trees, int64_t* offsets) {
+  if (!t) return fail(CKD_ERR_BAD_ARG, "null tree handle");
+  if (n_trees) *n_trees = t->n_trees;
+  if (offsets) std::memcpy(offsets, t->tree_off.data(), sizeof(int64_t) * t->tree_off.size());
+  return CKD_OK;
+}
+
+ckd_status ckd_forest_knn(const ckd_tree* t, const double* q, const int64_t* q_offsets, int64_t nq,
+                          int k, int sorted, double* dist, int64_t* idx, void* stream) {
+  CKD_TRY(check_forest(t));
+  if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !q_offsets || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query, offset or output pointer");
+  if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* qroot = nullptr;
+  CKD_CUDA(dev_alloc((void**)&qroot, sizeof(int32_t) * nq, s));
+  ckd_status st = csr_owner(q_offsets, (int32_t)t->n_trees, nq, qroot, s);
+  if (st == CKD_OK) st = forest_knn(t, q, qroot, nq, k, sorted, dist, idx, s);
+  dev_free(qroot, s);
+  return st;
+}
+
+static ckd_status forest_box(const ckd_tree* t, const double* boxes, const int64_t* b_offsets,
+                             int64_t nb, bool fill, int64_t* counts, const int64_t* offsets,
+                             int64_t* idx, void* stream) {
+  CKD_TRY(check_forest(t));
+  if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
+  if (nb == 0) return CKD_OK;
+  if (!boxes || !b_offsets || (fill ? (!offsets || !idx) : !counts))
+    return fail(CKD_ERR_BAD_ARG, "null box, offset or output pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* broot = nullptr;
+  CKD_CUDA(dev_alloc((void**)&broot, sizeof(int32_t) * nb, s));
+  ckd_status st = csr_owner(b_offsets, (int32_t)t->n_trees, nb, broot, s);
+  if (st == CKD_OK) st = box_run(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+  dev_free(broot, s);
+  return st;
+}
+
+ckd_status ckd_forest_box_count(const ckd_tree* t, const double* boxes, const int64_t* b_offsets,
+                                int64_t nb, int64_t* counts, void* stream) {
+  return forest_box(t, boxes, b_offsets, nb, false, counts, nullptr, nullptr, stream);
+}
+
+ckd_status ckd_forest_box_fill(const ckd_tree* t, const double* boxes, const int64_t* b_offsets,
+                               int64_t nb, const int64_t* offsets, int64_t* idx, void* stream) {
+  return forest_box(t, boxes, b_offsets, nb, true, nullptr, offsets, idx, stream);
+}
+
 ckd_status ckd_free(ckd_tree* tree) {
   if (!tree) return CKD_OK;
   int cur = 0;
@@ -238,7 +334,7 @@ ckd_status ckd_tree_info(const ckd_tree* t, int64_t* n, int* d, int* leaf, int* 
 ckd_status ckd_tree_export(const ckd_tree* t, int32_t* axis, double* split, int64_t* start,
                            int64_t* count, int64_t* left, int64_t* right, double* cell, double* box,
                            int64_t* ids) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   const int m = t->n_nodes, d2 = 2 * t->d;
   std::vector<NodeMeta> meta(m);
   std::vector<double> hc((size_t)m * d2), hb((size_t)m * d2);
@@ -283,7 +379,7 @@ ckd_status ckd_tree_export(const ckd_tree* t, int32_t* axis, double* split, int6
 
 ckd_status ckd_knn(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;
@@ -293,7 +389,7 @@ ckd_status ckd_knn(const ckd_tree* t, const double* q, int64_t nq, int k, int so
 
 ckd_status ckd_query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
                            void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;
   if (!q || !order) return fail(CKD_ERR_BAD_ARG, "null query or order pointer");
@@ -302,7 +398,7 @@ ckd_status ckd_query_order(const ckd_tree* t, const double* q, int64_t nq, int32
 
 ckd_status ckd_knn_ordered(const ckd_tree* t, const double* q, int64_t nq, const int32_t* order,
                            int k, int sorted, double* dist, int64_t* idx, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;
@@ -363,7 +459,7 @@ ckd_status ckd_set_tuning(int key, int value) {
 
 ckd_status ckd_knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                            double* dist, int64_t* idx, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;
@@ -374,7 +470,7 @@ ckd_status ckd_knn_noalloc(const ckd_tree* t, const double* q, int64_t nq, int k
 ckd_status ckd_knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq,
                            int k, int sorted, double* dist, int64_t* idx, int64_t* n_fallback,
                            void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   CKD_TRY(mlp_check(net));
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
@@ -387,7 +483,7 @@ ckd_status ckd_knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* 
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                         double* dist, int64_t* idx, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;
@@ -413,7 +509,7 @@ ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, i
 
 ckd_status ckd_ball_count(const ckd_tree* t, const double* q, int64_t nq, double radius,
                           int64_t* counts, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (!(radius > 0) || !std::isfinite(radius))
     return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
@@ -425,7 +521,7 @@ ckd_status ckd_ball_count(const ckd_tree* t, const double* q, int64_t nq, double
 
 ckd_status ckd_ball_fill(const ckd_tree* t, const double* q, int64_t nq, double radius, int sorted,
                          const int64_t* offsets, int64_t* idx, double* dist, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (!(radius > 0) || !std::isfinite(radius))
     return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
@@ -437,7 +533,7 @@ ckd_status ckd_ball_fill(const ckd_tree* t, const double* q, int64_t nq, double 
 
 ckd_status ckd_box_count(const ckd_tree* t, const double* boxes, int64_t nb, int64_t* counts,
                          void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
   if (nb == 0) return CKD_OK;
   if (!boxes || !counts) return fail(CKD_ERR_BAD_ARG, "null box or output pointer");
@@ -446,7 +542,7 @@ ckd_status ckd_box_count(const ckd_tree* t, const double* boxes, int64_t nb, int
 
 ckd_status ckd_box_fill(const ckd_tree* t, const double* boxes, int64_t nb, const int64_t* offsets,
                         int64_t* idx, void* stream) {
-  CKD_TRY(check_tree(t));
+  CKD_TRY(check_single(t));
   if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
   if (nb == 0) return CKD_OK;
   if (!boxes || !offsets || !idx) return fail(CKD_ERR_BAD_ARG, "null box or output pointer");

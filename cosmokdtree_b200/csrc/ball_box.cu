@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restri
                                              int64_t nb, int32_t* __restrict__ gstack,
                                              int stack_len, int64_t* __restrict__ counts,
                                              const int64_t* __restrict__ offsets,
-                                             int64_t* __restrict__ oidx) {
+                                             int64_t* __restrict__ oidx,
+                                             const int32_t* __restrict__ broot) {
   __shared__ int32_t snode[4][kStack];
   __shared__ unsigned smask[4][kStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -172,7 +173,19 @@ __global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restri
   int64_t cur = (FILL && valid) ? offsets[bi] : 0;
   const int64_t cur_end = (FILL && valid) ? offsets[bi + 1] : 0;
   int top = 0;
-  if (lane == 0) {
+  if (broot) {
+    // forest: one start entry per distinct tree among the warp's boxes
+    const int32_t r = valid ? broot[bi] : -1;
+    const unsigned same = __match_any_sync(0xffffffffu, r);
+    const bool leader = valid && (__ffs(same) - 1) == lane;
+    const unsigned lead = __ballot_sync(0xffffffffu, leader);
+    if (leader) {
+      const int slot = __popc(lead & (bit - 1u));
+      stn[slot] = r;
+      stm[slot] = same;
+    }
+    top = __popc(lead) - 1;
+  } else if (lane == 0) {
     stn[0] = 0;
     stm[0] = vm;
   }
@@ -261,21 +274,23 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
 
 template <int D>
 ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool fill,
-                      int64_t* counts, const int64_t* offsets, int64_t* idx, cudaStream_t s) {
+                      int64_t* counts, const int64_t* offsets, int64_t* idx, cudaStream_t s,
+                      const int32_t* broot) {
   TreeView tv = t->view();
   const int threads = 128, nw = threads / 32;
   int64_t warps = cdiv(nb, 32);
   unsigned blocks = (unsigned)cdiv(warps, nw);
-  int stack_len = std::max(kStack, t->depth + 4);
+  // a packet stack grows by at most one entry per level past its start entries
+  int stack_len = std::max(kStack, t->depth + 4 + (broot ? 32 : 0));
   int32_t* gstack = nullptr;
   if (stack_len > kStack)
     CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw, s));
   if (fill)
     k_box<D, true><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, nullptr, offsets,
-                                              idx);
+                                              idx, broot);
   else
     k_box<D, false><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, counts, nullptr,
-                                               nullptr);
+                                               nullptr, broot);
   CKD_LAUNCH_CHECK();
   if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
@@ -318,16 +333,16 @@ ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bo
 }
 
 ckd_status box_run(const ckd_tree* t, const double* boxes, int64_t nb, bool fill, int64_t* counts,
-                   const int64_t* offsets, int64_t* idx, cudaStream_t s) {
+                   const int64_t* offsets, int64_t* idx, cudaStream_t s, const int32_t* broot) {
   switch (t->d) {
-    case 1: return box_launch<1>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 2: return box_launch<2>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 3: return box_launch<3>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 4: return box_launch<4>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 5: return box_launch<5>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 6: return box_launch<6>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 7: return box_launch<7>(t, boxes, nb, fill, counts, offsets, idx, s);
-    case 8: return box_launch<8>(t, boxes, nb, fill, counts, offsets, idx, s);
+    case 1: return box_launch<1>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 2: return box_launch<2>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 3: return box_launch<3>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 4: return box_launch<4>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 5: return box_launch<5>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 6: return box_launch<6>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 7: return box_launch<7>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
+    case 8: return box_launch<8>(t, boxes, nb, fill, counts, offsets, idx, s, broot);
   }
   return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
 }

@@ -64,16 +64,29 @@ struct BuildBufs {
 
 // ------------------------------------------------------------------ kernels
 
-// row-major (n x d) FP64/FP32 -> SoA FP64, ids = 0..n-1, NID[0] = 0, NID[1] = -1
+// row-major (n x d) FP64/FP32 -> SoA FP64.  Tree t of a forest owns positions
+// [off[t], off[t+1]) and is rooted at node t; ids are local to their tree
+// (0..n_t-1), NID[0] = the tree's root, NID[1] = -1.  off == nullptr: one tree.
 template <typename T>
 __global__ void k_init_points(const T* __restrict__ in, int64_t n, int d, double* __restrict__ X,
                               int32_t* __restrict__ I, int32_t* __restrict__ N0,
-                              int32_t* __restrict__ N1) {
+                              int32_t* __restrict__ N1, const int64_t* __restrict__ off,
+                              int32_t n_trees) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   for (int j = 0; j < d; ++j) X[(int64_t)j * n + p] = (double)in[p * d + j];
-  I[p] = (int32_t)p;
-  N0[p] = 0;
+  int32_t t = 0;
+  if (off) {  // last tree with off[t] <= p
+    int32_t lo = 0, hi = n_trees - 1;
+    while (lo < hi) {
+      int32_t mid = (lo + hi + 1) >> 1;
+      if (off[mid] <= p) lo = mid;
+      else hi = mid - 1;
+    }
+    t = lo;
+  }
+  I[p] = (int32_t)(p - (off ? off[t] : 0));
+  N0[p] = t;
   N1[p] = -1;
 }
 
@@ -197,7 +210,7 @@ template <int D>
 __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
                          double* __restrict__ cell, double* __restrict__ box,
                          const unsigned long long* __restrict__ keys, int32_t* __restrict__ mode,
-                         int32_t* __restrict__ ext, int root_cell_from_box) {
+                         int32_t* __restrict__ ext) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int32_t a = act[i];
@@ -208,13 +221,6 @@ __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __res
     hi[j] = dkey_inv(keys[(int64_t)a * 2 * D + 2 * j + 1]);
     box[(int64_t)a * 2 * D + 2 * j] = lo[j];
     box[(int64_t)a * 2 * D + 2 * j + 1] = hi[j];
-  }
-  if (root_cell_from_box && a == 0) {  // cosmokdtree.f90:226-229
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-      cell[2 * j] = lo[j];
-      cell[2 * j + 1] = hi[j];
-    }
   }
 #pragma unroll
   for (int j = 0; j < D; ++j) {
@@ -528,24 +534,37 @@ __global__ void k_search_records(const NodeMeta* __restrict__ meta, int32_t n_no
   rec[4 * NV] = *reinterpret_cast<float4*>(&info);
 }
 
+// roots: node t = root of tree t (positions off[t] .. off[t+1]-1)
 template <int D>
-__global__ void k_root_init(NodeMeta* meta, double* cell, unsigned long long* keys, int32_t n,
-                            const double* L, int periodic) {
+__global__ void k_root_init(NodeMeta* meta, double* cell, unsigned long long* keys,
+                            const int64_t* __restrict__ off, int32_t n_trees, const double* L,
+                            int periodic) {
+  int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_trees) return;
   NodeMeta m;
   m.split = 0.0;
   m.left = -1;
   m.axis = -1;
-  m.start = 0;
-  m.count = n;
+  m.start = (int32_t)off[t];
+  m.count = (int32_t)(off[t + 1] - off[t]);
   m.depth = 0;
   m.parent = -1;
-  meta[0] = m;
+  meta[t] = m;
   for (int j = 0; j < D; ++j) {
-    cell[2 * j] = periodic ? -L[j] / 2. : 0.0;  // :218-224 (every axis)
-    cell[2 * j + 1] = periodic ? L[j] / 2. : 0.0;
-    keys[2 * j] = ~0ull;
-    keys[2 * j + 1] = 0ull;
+    cell[(int64_t)t * 2 * D + 2 * j] = periodic ? -L[j] / 2. : 0.0;  // :218-224 (every axis)
+    cell[(int64_t)t * 2 * D + 2 * j + 1] = periodic ? L[j] / 2. : 0.0;
+    keys[(int64_t)t * 2 * D + 2 * j] = ~0ull;
+    keys[(int64_t)t * 2 * D + 2 * j + 1] = 0ull;
   }
+}
+
+// non-periodic root cells = the data bounding box of each tree (:226-229)
+template <int D>
+__global__ void k_root_cells(double* cell, const unsigned long long* __restrict__ keys,
+                             int32_t n_trees) {
+  int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_trees) return;
+  for (int j = 0; j < 2 * D; ++j) cell[(int64_t)t * 2 * D + j] = dkey_inv(keys[(int64_t)t * 2 * D + j]);
 }
 
 // ------------------------------------------------------------------ host side
@@ -611,7 +630,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     CKD_CUDA(dev_alloc((void**)&B.I[b], sizeof(int32_t) * n, s));
     CKD_CUDA(dev_alloc((void**)&B.NID[b], sizeof(int32_t) * n, s));
   }
-  int64_t max_open = n / (leaf + 1) + 2;
+  int64_t max_open = n / (leaf + 1) + 2 + t->n_trees;
   for (int b = 0; b < 2; ++b) CKD_CUDA(dev_alloc((void**)&B.act[b], sizeof(int32_t) * max_open, s));
   CKD_CUDA(dev_alloc((void**)&B.nxt_cnt, sizeof(int32_t) * max_open, s));
   CKD_CUDA(dev_alloc((void**)&B.nxt_off, sizeof(int32_t) * (max_open + 1), s));
@@ -619,72 +638,94 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
   CKD_CUDA(cudaMemsetAsync(B.scal, 0, sizeof(int32_t) * 4, s));
-  CKD_TRY(ensure_node_cap(B, std::max<int64_t>(64, 4 * (n / std::max(1, leaf)) + 64), s));
 
   // final outputs
   CKD_CUDA(cudaMalloc((void**)&t->pts, sizeof(double) * D * n));
   CKD_CUDA(cudaMalloc((void**)&t->ids, sizeof(int32_t) * n));
 
+  // trees of a forest: positions off[t] .. off[t+1]-1, root node t
+  const int32_t T = (int32_t)t->n_trees;
+  const std::vector<int64_t>& off = t->tree_off;
+  int64_t* off_dev = nullptr;
+  CKD_CUDA(dev_alloc((void**)&off_dev, sizeof(int64_t) * (T + 1), s));
+  CKD_CUDA(cudaMemcpyAsync(off_dev, off.data(), sizeof(int64_t) * (T + 1), cudaMemcpyHostToDevice, s));
   {
     unsigned g = (unsigned)cdiv(n, 256);
+    const int64_t* offp = T > 1 ? off_dev : nullptr;
     if (dtype == CKD_F32)
       k_init_points<float><<<g, 256, 0, s>>>((const float*)pts_dev, n, D, B.X[0], B.I[0],
-                                             B.NID[0], B.NID[1]);
+                                             B.NID[0], B.NID[1], offp, T);
     else
       k_init_points<double><<<g, 256, 0, s>>>((const double*)pts_dev, n, D, B.X[0], B.I[0],
-                                              B.NID[0], B.NID[1]);
+                                              B.NID[0], B.NID[1], offp, T);
     CKD_LAUNCH_CHECK();
   }
   double* Ldev = nullptr;
   CKD_CUDA(dev_alloc((void**)&Ldev, sizeof(double) * CKD_MAX_D, s));
   CKD_CUDA(cudaMemcpyAsync(Ldev, t->L, sizeof(double) * CKD_MAX_D, cudaMemcpyHostToDevice, s));
-  k_root_init<D><<<1, 1, 0, s>>>(B.meta, B.cell, B.keys, (int32_t)n, Ldev, t->periodic);
+  CKD_TRY(ensure_node_cap(B, (int64_t)T + std::max<int64_t>(64, 4 * (n / std::max(1, leaf)) + 64), s));
+  k_root_init<D><<<(unsigned)cdiv(T, 128), 128, 0, s>>>(B.meta, B.cell, B.keys, off_dev, T, Ldev,
+                                                        t->periodic);
   CKD_LAUNCH_CHECK();
-  int32_t root = 0;
-  CKD_CUDA(cudaMemcpyAsync(B.act[0], &root, sizeof(int32_t), cudaMemcpyHostToDevice, s));
 
-  // Root bounding box: validation (finite, inside the periodic box) and the
-  // non-periodic root cell.  Computed with the open-node reduction using a leaf
-  // threshold of 0 so that the root is always "open" here.
+  // Root bounding boxes: validation (finite, inside the periodic box) and the
+  // non-periodic root cells.  Computed with the open-node reduction using a leaf
+  // threshold of 0 so that every root is "open" here.
   k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], B.meta, 0, 0, n, B.keys);
   CKD_LAUNCH_CHECK();
-  unsigned long long rk[2 * CKD_MAX_D];
-  CKD_CUDA(cudaMemcpyAsync(rk, B.keys, sizeof(unsigned long long) * 2 * D, cudaMemcpyDeviceToHost, s));
+  std::vector<unsigned long long> rk((size_t)T * 2 * D);
+  CKD_CUDA(cudaMemcpyAsync(rk.data(), B.keys, sizeof(unsigned long long) * 2 * D * T,
+                           cudaMemcpyDeviceToHost, s));
   CKD_CUDA(cudaStreamSynchronize(s));
   double rlo[CKD_MAX_D], rhi[CKD_MAX_D];
   for (int j = 0; j < D; ++j) {
-    auto inv = [](unsigned long long k) {
-      unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
-      double x;
-      std::memcpy(&x, &b, 8);
-      return x;
-    };
-    rlo[j] = inv(rk[2 * j]);
-    rhi[j] = inv(rk[2 * j + 1]);
-    if (!std::isfinite(rlo[j]) || !std::isfinite(rhi[j]))
-      return fail(CKD_ERR_BAD_ARG, "points contain NaN or infinite coordinates");
-    if (t->periodic && (rlo[j] < -t->L[j] / 2 || rhi[j] > t->L[j] / 2))
-      return fail(CKD_ERR_OUT_OF_BOX, "Points outside (-L/2, L/2) range");
+    rlo[j] = INFINITY;
+    rhi[j] = -INFINITY;
   }
-
-  int32_t n_nodes = 1;
-  int m = n > leaf ? 1 : 0;
-  int cur = 0;
-  int level = 0;
-  int root_from_box = t->periodic ? 0 : 1;
-  if (m == 0) {
-    // the root is a leaf: points stay in input order
-    CKD_CUDA(cudaMemcpyAsync(t->pts, B.X[0], sizeof(double) * D * n, cudaMemcpyDeviceToDevice, s));
-    CKD_CUDA(cudaMemcpyAsync(t->ids, B.I[0], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
-    if (root_from_box) {
-      double c[2 * CKD_MAX_D];
-      for (int j = 0; j < D; ++j) {
-        c[2 * j] = rlo[j];
-        c[2 * j + 1] = rhi[j];
+  for (int32_t tr = 0; tr < T; ++tr) {
+    for (int j = 0; j < D; ++j) {
+      auto inv = [](unsigned long long k) {
+        unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double x;
+        std::memcpy(&x, &b, 8);
+        return x;
+      };
+      double lo = inv(rk[(size_t)tr * 2 * D + 2 * j]), hi = inv(rk[(size_t)tr * 2 * D + 2 * j + 1]);
+      if (!std::isfinite(lo) || !std::isfinite(hi)) {
+        dev_free(Ldev, s);
+        dev_free(off_dev, s);
+        return fail(CKD_ERR_BAD_ARG, "points contain NaN or infinite coordinates");
       }
-      CKD_CUDA(cudaMemcpyAsync(B.cell, c, sizeof(double) * 2 * D, cudaMemcpyHostToDevice, s));
+      if (t->periodic && (lo < -t->L[j] / 2 || hi > t->L[j] / 2)) {
+        dev_free(Ldev, s);
+        dev_free(off_dev, s);
+        return fail(CKD_ERR_OUT_OF_BOX, "Points outside (-L/2, L/2) range");
+      }
+      rlo[j] = std::min(rlo[j], lo);
+      rhi[j] = std::max(rhi[j], hi);
     }
   }
+  if (!t->periodic) {
+    k_root_cells<D><<<(unsigned)cdiv(T, 128), 128, 0, s>>>(B.cell, B.keys, T);
+    CKD_LAUNCH_CHECK();
+  }
+  // points of trees that are a single leaf never move: start from the input order
+  CKD_CUDA(cudaMemcpyAsync(t->pts, B.X[0], sizeof(double) * D * n, cudaMemcpyDeviceToDevice, s));
+  CKD_CUDA(cudaMemcpyAsync(t->ids, B.I[0], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+  // open roots
+  std::vector<int32_t> roots;
+  for (int32_t tr = 0; tr < T; ++tr)
+    if (off[tr + 1] - off[tr] > leaf) roots.push_back(tr);
+  if (!roots.empty())
+    CKD_CUDA(cudaMemcpyAsync(B.act[0], roots.data(), sizeof(int32_t) * roots.size(),
+                             cudaMemcpyHostToDevice, s));
+  CKD_CUDA(cudaStreamSynchronize(s));  // `roots` and `rk` are host buffers of the copies
+  dev_free(off_dev, s);
+
+  int32_t n_nodes = T;
+  int m = (int)roots.size();
+  int cur = 0;
+  int level = 0;
   while (m > 0) {
     if (level >= kMaxLevels) {
       dev_free(Ldev, s);
@@ -698,8 +739,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
                                                     B.keys);
       CKD_LAUNCH_CHECK();
     }
-    k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext,
-                                   level == 0 ? root_from_box : 0);
+    k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
     CKD_LAUNCH_CHECK();
     k_argext<<<(unsigned)cdiv(n, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, level,
                                                     leaf, n, B.ext);
@@ -767,8 +807,8 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_LAUNCH_CHECK();
   CKD_CUDA(cudaStreamSynchronize(s));
   if (err) return fail(CKD_ERR_CUDA, "internal error: inconsistent partition in build");
-  // leaves = (nodes + 1) / 2 for a full binary tree
-  t->n_leaves = (n_nodes + 1) / 2;
+  // leaves = (nodes + 1) / 2 for each full binary tree
+  t->n_leaves = (n_nodes + T) / 2;
   return CKD_OK;
 }
 

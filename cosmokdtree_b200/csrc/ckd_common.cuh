@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include <cfloat>
 #include <string>
+#include <vector>
 
 #include "../../include/ckd.h"
 
@@ -159,6 +160,9 @@ ckd_status scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, cudaStrea
 ckd_status scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 // exclusive scan of n int32 values into int32 (out has n+1 entries)
 ckd_status scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
+// owner[i] = row t of CSR offsets off (n_rows + 1 entries) holding item i
+ckd_status csr_owner(const int64_t* off_dev, int32_t n_rows, int64_t n_items, int32_t* owner,
+                     cudaStream_t s);
 
 }  // namespace ckd
 
@@ -174,6 +178,10 @@ struct ckd_tree {
   int32_t n_nodes = 0;
   int32_t n_leaves = 0;
   int32_t depth = 0;
+  // a forest holds n_trees independent trees: tree t owns points
+  // tree_off[t] .. tree_off[t+1]-1 (ids local to the tree) and is rooted at node t
+  int64_t n_trees = 1;
+  std::vector<int64_t> tree_off;
   ckd::NodeMeta* meta = nullptr;
   double* box = nullptr;
   double* cell = nullptr;

@@ -566,7 +566,8 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
                                                   const double* __restrict__ r2 = nullptr,
                                                   int32_t* __restrict__ miss = nullptr,
                                                   unsigned* __restrict__ nmiss = nullptr,
-                                                  const int32_t* __restrict__ qleaf = nullptr) {
+                                                  const int32_t* __restrict__ qleaf = nullptr,
+                                                  const int32_t* __restrict__ qroot = nullptr) {
   constexpr int NV = (D + 3) / 4;
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -612,7 +613,8 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
   int32_t sn[kLaneStack];
   float sd[kLaneStack];
   int top = 0;
-  int32_t node = valid ? 0 : -1;
+  // a forest query starts at its own tree's root
+  int32_t node = valid ? (qroot ? qroot[qi] : 0) : -1;
   if (BOUNDED && valid && qleaf && sid == 0x7fffffff) {
     // Start at the lowest ancestor of the query's leaf whose cell strictly
     // contains the cube [q - r, q + r]^D: every point within the bound lies
@@ -621,7 +623,7 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
     // this conservative.
     const float r32 = __fsqrt_ru(wd32);
     int32_t a = qleaf[qi];
-    while (a > 0) {
+    while (a >= 0) {
       const float* c = tv.cell32 + (int64_t)a * 2 * D;
       bool inside = true;
 #pragma unroll
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
       if (inside) break;
       a = load_meta(tv.meta, a).parent;
     }
-    node = a < 0 ? 0 : a;
+    node = a < 0 ? node : a;
   }
   while (node >= 0) {
     // ---- descend to a leaf, nearer child first
@@ -2103,14 +2105,14 @@ __global__ void k_bucket_emit(const NodeMeta* __restrict__ meta, int32_t n_nodes
 template <int D>
 __global__ void k_locate(const NodeMeta* __restrict__ meta, const double* __restrict__ Q,
                          int64_t nq, int32_t* __restrict__ key, int32_t* __restrict__ hist,
-                         int32_t* __restrict__ qleaf) {
+                         int32_t* __restrict__ qleaf, const int32_t* __restrict__ qroot) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
   double q[D];
 #pragma unroll
   for (int j = 0; j < D; ++j) q[j] = Q[i * D + j];
-  int32_t node = 0;
-  NodeMeta m = load_meta(meta, 0);
+  int32_t node = qroot ? qroot[i] : 0;
+  NodeMeta m = load_meta(meta, node);
   while (m.left >= 0) {
     double qa = 0.0;
 #pragma unroll
@@ -2231,7 +2233,8 @@ ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* ord
 
 template <int D>
 ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                      int32_t* qleaf, cudaStream_t s, int32_t** off_out = nullptr) {
+                      int32_t* qleaf, cudaStream_t s, int32_t** off_out = nullptr,
+                      const int32_t* qroot = nullptr) {
   int64_t n = t->n;
   int32_t *key = nullptr, *hist = nullptr, *off = nullptr;
   CKD_CUDA(dev_alloc((void**)&key, sizeof(int32_t) * nq, s));
@@ -2239,7 +2242,7 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   CKD_CUDA(dev_alloc((void**)&off, sizeof(int32_t) * (n + 1), s));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   unsigned g = (unsigned)cdiv(nq, 256);
-  k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist, qleaf);
+  k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist, qleaf, qroot);
   CKD_LAUNCH_CHECK();
   CKD_TRY(scan_i32(hist, off, n, s));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
@@ -2391,6 +2394,61 @@ ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int so
   if (order) dev_free(order, s);
   if (qleaf) dev_free(qleaf, s);
   return st;
+}
+
+// ===================================================================
+// kNN over a forest (ckd_forest_knn): every query carries its tree (qroot =
+// the tree's root node); the queries of all trees are ordered by leaf and
+// searched by one per-lane launch that starts each lane at its own root.
+namespace {
+
+template <int D, bool PER>
+ckd_status forest_knn_impl(const ckd_tree* t, const double* q, const int32_t* qroot, int64_t nq,
+                           int k, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+  int32_t* order = nullptr;
+  CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
+  ckd_status st = order_impl<D>(t, q, nq, order, nullptr, s, nullptr, qroot);
+  if (st == CKD_OK) {
+    const int nw = knn_warps_per_block();
+    const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    const int bps = knn_blocks_per_sm();
+    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
+    cudaError_t e = cudaFuncSetAttribute(k_knn_lane<D, PER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) {
+      dev_free(order, s);
+      return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane)");
+    }
+    timing_begin(s);
+    k_knn_lane<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist, idx,
+                                                   knn_stats_buffer(), nullptr, nullptr, nullptr,
+                                                   nullptr, qroot);
+    note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) st = cuda_fail(e, "k_knn_lane (forest)");
+    else timing_end(s);
+  }
+  dev_free(order, s);
+  return st;
+}
+
+}  // namespace
+
+ckd_status forest_knn(const ckd_tree* t, const double* q, const int32_t* qroot, int64_t nq, int k,
+                      int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+  if (!(t->screen_ok && t->depth < kLaneStack - 1 && k <= kSmemK))
+    return fail(CKD_ERR_BAD_ARG,
+                "forest kNN needs k <= 64, trees shallower than 127 levels and coordinates "
+                "below 1e18");
+  switch (t->d * 2 + (t->periodic ? 1 : 0)) {
+#define CKD_FK(DD)                                                                        \
+  case 2 * DD: return forest_knn_impl<DD, false>(t, q, qroot, nq, k, sorted, dist, idx, s); \
+  case 2 * DD + 1: return forest_knn_impl<DD, true>(t, q, qroot, nq, k, sorted, dist, idx, s);
+    CKD_FK(1) CKD_FK(2) CKD_FK(3) CKD_FK(4) CKD_FK(5) CKD_FK(6) CKD_FK(7) CKD_FK(8)
+#undef CKD_FK
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
 }
 
 // ===================================================================

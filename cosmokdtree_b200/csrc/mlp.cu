@@ -636,6 +636,7 @@ ckd_status ckd_mlp_set(ckd_mlp* net, const float* params, const float* norm, flo
 ckd_status ckd_mlp_features(const ckd_tree* t, const double* q, int64_t nq, int k, float* feat,
                             void* stream) {
   if (!t) return fail(CKD_ERR_BAD_ARG, "null tree handle");
+  if (t->n_trees != 1) return fail(CKD_ERR_BAD_ARG, "features are defined for a single tree");
   if (k < 1) return fail(CKD_ERR_BAD_ARG, "k must be a positive integer");
   if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
   if (nq == 0) return CKD_OK;

@@ -81,6 +81,20 @@ ckd_status scan_impl(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
   return CKD_OK;
 }
 
+// owner[i] = the t with off[t] <= i < off[t+1] (CSR rows -> row index)
+__global__ void k_csr_owner(const int64_t* __restrict__ off, int32_t n_rows, int64_t n_items,
+                            int32_t* __restrict__ owner) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_items) return;
+  int32_t lo = 0, hi = n_rows - 1;
+  while (lo < hi) {
+    int32_t mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  owner[i] = lo;
+}
+
 }  // namespace
 
 ckd_status scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, cudaStream_t s) {
@@ -91,6 +105,14 @@ ckd_status scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s) 
 }
 ckd_status scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s) {
   return scan_impl<int32_t, int32_t>(in, out, n, s);
+}
+
+ckd_status csr_owner(const int64_t* off_dev, int32_t n_rows, int64_t n_items, int32_t* owner,
+                      cudaStream_t s) {
+  if (n_items <= 0) return CKD_OK;
+  k_csr_owner<<<(unsigned)cdiv(n_items, 256), 256, 0, s>>>(off_dev, n_rows, n_items, owner);
+  CKD_LAUNCH_CHECK();
+  return CKD_OK;
 }
 
 }  // namespace ckd

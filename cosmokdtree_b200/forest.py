@@ -1,0 +1,190 @@
+"""Forests: thousands of independent trees of uneven sizes built and searched together.
+
+Halo and subvolume catalogues come as many small, independent point sets.  The
+reference builds one tree per call (src/cosmokdtree/kdtree.py:16-34) and keeps
+the periodic box side in a module global (src/cosmokdtree.f90:87); here all
+trees are built by one level-synchronous pass over every tree at once and all
+trees' queries go through one ordering pass and one search launch
+(``ckd_forest_*`` in include/ckd.h).  Every tree is exactly the tree
+``build_kdtree`` would make from its own points, and every result equals the
+single-tree result, with ids local to the tree.
+
+    forest = build_forest(points, offsets, leaf=16, boxsize=1.0)
+    dist, idx = forest.knn(queries, query_offsets, k=8)      # CUDA tensors
+    offs, ids = forest.box_csr(boxes, box_offsets)
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import CKDArgumentError, check
+from .kdtree import _check_k, _on_device, _ptr, _stream
+
+__all__ = ["Forest", "build_forest"]
+
+
+def _offsets(off, n_trees=None, total=None, what="offsets") -> np.ndarray:
+    o = np.asarray(off.cpu() if isinstance(off, torch.Tensor) else off, dtype=np.int64).reshape(-1)
+    if o.size < 2 or o[0] != 0 or np.any(np.diff(o) < 0):
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, f"{what} must start at 0 and not decrease")
+    if n_trees is not None and o.size != n_trees + 1:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, f"{what} must have n_trees + 1 entries")
+    if total is not None and o[-1] != total:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, f"{what}[-1] must equal the number of rows")
+    return np.ascontiguousarray(o)
+
+
+def _rows(x, d, device, name):
+    if isinstance(x, (list, tuple)):
+        x = np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1, d) for a in x]) \
+            if len(x) else np.zeros((0, d))
+    t = x.to(device=f"cuda:{device}", dtype=torch.float64) if _on_device(x) else \
+        torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.float64)))
+    if t.dim() != 2 or t.shape[1] != d:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM, f"{name} must be (n, {d})")
+    if not t.is_cuda:
+        t = t.pin_memory().to(f"cuda:{device}", non_blocking=True)
+    return t.contiguous()
+
+
+class Forest:
+    """Handle of a forest built on one GPU (owns all device buffers)."""
+
+    def __init__(self, handle, offsets, d, leaf, boxsize, device):
+        self._h = handle
+        self.offsets = offsets
+        self.n_trees = len(offsets) - 1
+        self.n = int(offsets[-1])
+        self.d = d
+        self.leaf = leaf
+        self.boxsize = boxsize
+        self.periodic = boxsize is not None
+        self.device = device
+        info = [ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()]
+        check(_lib.load().ckd_tree_info(self._h, None, None, None, None, ctypes.byref(info[0]),
+                                        ctypes.byref(info[1]), ctypes.byref(info[2]), None))
+        self.n_nodes, self.n_leaves, self.depth = (int(x.value) for x in info)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "forest has been deallocated")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.load().ckd_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _grouped(self, x, off, name, width):
+        x = _rows(x, width, self.device, name)
+        o = _offsets(off, self.n_trees, x.shape[0], f"{name} offsets")
+        if name == "queries" and self.periodic and x.shape[0] > 0:
+            half = torch.as_tensor(self.boxsize / 2.0, dtype=torch.float64, device=x.device)
+            if bool(((x < -half) | (x > half) | torch.isnan(x)).any()):
+                raise CKDArgumentError(_lib.CKD_ERR_OUT_OF_BOX,
+                                       "periodic forest: query points must lie in [-L/2, L/2]")
+        return x, torch.from_numpy(o).to(f"cuda:{self.device}")
+
+    def knn(self, queries, query_offsets, k, sorted=True):
+        """kNN of queries grouped by tree (rows query_offsets[t] .. [t+1]-1 search
+        tree t).  Returns (dist, idx) CUDA tensors (nq, k); ids local to the tree."""
+        k = _check_k(k)
+        with torch.cuda.device(self.device):
+            q, qo = self._grouped(queries, query_offsets, "queries", self.d)
+            return self.knn_device(q, qo, k, sorted)
+
+    def knn_device(self, q: torch.Tensor, q_offsets: torch.Tensor, k: int, sorted=True,
+                   out=None):
+        """As ``knn`` with inputs already on the device (float64 (nq, d) and int64
+        offsets) and optional preallocated outputs; does not synchronise, so it can
+        be captured in a CUDA graph."""
+        nq = q.shape[0]
+        if out is None:
+            dist = torch.empty((nq, k), dtype=torch.float64, device=q.device)
+            idx = torch.empty((nq, k), dtype=torch.int64, device=q.device)
+        else:
+            dist, idx = out
+        if nq > 0:
+            check(_lib.load().ckd_forest_knn(self.handle, _ptr(q), _ptr(q_offsets), nq, int(k),
+                                             int(bool(sorted)), _ptr(dist), _ptr(idx), _stream()))
+        return dist, idx
+
+    def box_csr(self, boxes, box_offsets):
+        """Points inside each box ([lo0, hi0, lo1, hi1, ...] rows, grouped by tree
+        like the kNN queries), as CSR CUDA tensors (offsets (nb+1,), idx)."""
+        L = _lib.load()
+        with torch.cuda.device(self.device):
+            b, bo = self._grouped(boxes, box_offsets, "boxes", 2 * self.d)
+            nb = b.shape[0]
+            counts = torch.empty(nb, dtype=torch.int64, device=b.device)
+            offsets = torch.zeros(nb + 1, dtype=torch.int64, device=b.device)
+            if nb > 0:
+                check(L.ckd_forest_box_count(self.handle, _ptr(b), _ptr(bo), nb, _ptr(counts),
+                                             _stream()))
+                check(L.ckd_exclusive_scan(_ptr(counts), _ptr(offsets), nb, _stream()))
+            total = int(offsets[-1].item())
+            idx = torch.empty(total, dtype=torch.int64, device=b.device)
+            if nb > 0 and total > 0:
+                check(L.ckd_forest_box_fill(self.handle, _ptr(b), _ptr(bo), nb, _ptr(offsets),
+                                            _ptr(idx), _stream()))
+        return offsets, idx
+
+
+def build_forest(points, offsets=None, leaf=16, boxsize=None) -> Forest:
+    """Build every tree of a forest in one pass.  ``points`` is an (N, d) array
+    (numpy or CUDA tensor) with ``offsets`` (n_trees + 1 row offsets), or a list of
+    per-tree (n_t, d) arrays.  All trees share ``leaf`` and ``boxsize`` (None: not
+    periodic; otherwise coordinates in [-L/2, L/2])."""
+    if leaf is None:
+        leaf = 16
+    if not (int(leaf) == leaf and leaf > 0):
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "Leaf size must be a positive integer")
+    leaf = int(leaf)
+    if isinstance(points, (list, tuple)):
+        sizes = [len(a) for a in points]
+        d = np.asarray(points[0]).shape[1]
+        pts = torch.from_numpy(np.ascontiguousarray(
+            np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1, d) for a in points])))
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    else:
+        pts = points if _on_device(points) else torch.from_numpy(
+            np.ascontiguousarray(np.asarray(points, dtype=np.float64)))
+        if offsets is None:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "offsets are required with an (N, d) array")
+        off = _offsets(offsets, total=pts.shape[0])
+    if pts.dim() != 2:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM, "points must be an (n, d) array")
+    n, d = pts.shape
+    if np.any(np.diff(off) <= 0):
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "every tree needs at least one point")
+    box = None
+    if boxsize is not None:
+        box = np.full(d, float(boxsize)) if np.ndim(boxsize) == 0 else \
+            np.array(boxsize, dtype=np.float64)
+        if len(box) != d:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM, "boxsize must have d entries")
+    if pts.dtype not in (torch.float32, torch.float64):
+        pts = pts.to(torch.float64)
+    dtype = _lib.CKD_F32 if pts.dtype == torch.float32 else _lib.CKD_F64
+    device = pts.device.index if pts.is_cuda else torch.cuda.current_device()
+    with torch.cuda.device(device):
+        if not pts.is_cuda:
+            pts = pts.pin_memory().to(f"cuda:{device}", non_blocking=True)
+        pts = pts.contiguous()
+        h = ctypes.c_void_p()
+        boxp = box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if box is not None else None
+        check(_lib.load().ckd_forest_build(
+            _ptr(pts), off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(off) - 1, d, dtype,
+            leaf, boxp, 1, _stream(), ctypes.byref(h)))
+    return Forest(h, off, d, leaf, box, device)

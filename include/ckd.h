@@ -170,6 +170,39 @@ ckd_status ckd_box_count(const ckd_tree* tree, const double* boxes_dev, int64_t 
 ckd_status ckd_box_fill(const ckd_tree* tree, const double* boxes_dev, int64_t nb,
                         const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Forests: many independent trees of uneven sizes built and searched together
+ * (halo / subvolume catalogues).  No single-call counterpart in the reference,
+ * which builds one tree per call (src/cosmokdtree.f90:124-238) and keeps the box
+ * side in a module global (src/cosmokdtree.f90:87), so each tree here is
+ * exactly the tree ckd_build would make from its points.
+ *
+ * Tree t owns rows offsets[t] .. offsets[t+1]-1 of pts (host array of n_trees+1
+ * entries, offsets[0] = 0, every tree non-empty); all trees share d, leaf and
+ * boxsize.  The result is a ckd_tree handle holding all trees; single-tree
+ * entry points reject it.  Ids in results are local to their tree (0-based). */
+ckd_status ckd_forest_build(const void* pts, const int64_t* offsets_host, int64_t n_trees, int d,
+                            int dtype, int leaf, const double* boxsize, int pts_on_device,
+                            void* stream, ckd_tree** out);
+/* Number of trees and (if not NULL) their host offsets (n_trees + 1 entries). */
+ckd_status ckd_forest_info(const ckd_tree* forest, int64_t* n_trees, int64_t* offsets_host);
+/* kNN of queries grouped by tree: queries q_offsets_dev[t] .. q_offsets_dev[t+1]-1
+ * (device array, n_trees + 1 entries) search tree t.  Results as ckd_knn, rows in
+ * query order.  All trees' queries go through one ordering pass and one search
+ * launch; no host synchronisation, so the call can be captured in a CUDA graph
+ * (after a first uncaptured call has set the kernel attributes).  Needs k <= 64. */
+ckd_status ckd_forest_knn(const ckd_tree* forest, const double* q_dev, const int64_t* q_offsets_dev,
+                          int64_t nq, int k, int sorted, double* dist_dev, int64_t* idx_dev,
+                          void* stream);
+/* Box search over a forest, boxes grouped by tree like the kNN queries
+ * (b_offsets_dev, device, n_trees + 1 entries); two-phase CSR as ckd_box_*. */
+ckd_status ckd_forest_box_count(const ckd_tree* forest, const double* boxes_dev,
+                                const int64_t* b_offsets_dev, int64_t nb, int64_t* counts_dev,
+                                void* stream);
+ckd_status ckd_forest_box_fill(const ckd_tree* forest, const double* boxes_dev,
+                               const int64_t* b_offsets_dev, int64_t nb,
+                               const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
+
 /* out_dev[0] = 0, out_dev[i+1] = in_dev[0] + ... + in_dev[i]  (n+1 outputs). */
 ckd_status ckd_exclusive_scan(const int64_t* in_dev, int64_t* out_dev, int64_t n, void* stream);
 

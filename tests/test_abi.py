@@ -66,3 +66,26 @@ def test_python_validation_before_device():
         kdtree._check_k(2.0)
     with pytest.raises(AssertionError):
         kdtree._check_radius(0.0)
+
+
+def test_forest_validation_without_gpu(lib):
+    """Forest offsets are validated on the host before any device work."""
+    from cosmokdtree_b200 import _lib
+    import numpy as np
+    P = np.zeros((100, 3))
+    h = ctypes.c_void_p()
+    pp = P.ctypes.data_as(ctypes.c_void_p)
+
+    def build(off, nt):
+        o = np.asarray(off, np.int64)
+        return lib.ckd_forest_build(pp, o.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), nt, 3,
+                                    0, 16, None, 0, None, ctypes.byref(h))
+
+    assert build([0, 50, 50, 100], 3) == _lib.CKD_ERR_BAD_ARG  # empty tree
+    assert "at least one point" in _lib.last_error()
+    assert build([1, 50, 100], 2) == _lib.CKD_ERR_BAD_ARG      # must start at 0
+    assert build([0, 100], 0) == _lib.CKD_ERR_BAD_ARG          # no trees
+    assert lib.ckd_forest_build(pp, None, 2, 3, 0, 16, None, 0, None,
+                                ctypes.byref(h)) == _lib.CKD_ERR_BAD_ARG
+    n = ctypes.c_int64()
+    assert lib.ckd_forest_info(None, ctypes.byref(n), None) == _lib.CKD_ERR_BAD_ARG
