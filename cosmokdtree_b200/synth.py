@@ -12,7 +12,8 @@ generators stand in for them:
   the NFW enclosed-mass CDF inverted by bisection, isotropic directions, wrapped
   periodically) plus 30% uniform background.
 * ``nfw_cluster``: one NFW-like cluster centred in its own periodic box (batched
-  trees configuration).
+  trees configuration); ``forest_catalogue`` draws a whole forest of them (tree
+  sizes log-uniform, concentration U(4, 20) per tree) on the GPU.
 * ``phase_space``: positions as in ``clustered_periodic`` but non-periodic, with
   velocities per cluster ~ N(v_bulk, sigma^2), sigma ~ U(0.05, 0.3),
   v_bulk ~ N(0, 0.1^2); background velocities N(0, 0.1^2).
@@ -115,3 +116,38 @@ def mixed_queries(P, nq, seed, box=1.0):
     q2 = (rng.random((nq - h, P.shape[1])) - 0.5) * box
     Q = np.concatenate([q1, q2])
     return np.ascontiguousarray(Q[rng.permutation(nq)])
+
+
+def forest_catalogue(n_trees, seed=2, n_range=(1e3, 1e6), c_range=(4.0, 20.0), rvir=0.25,
+                     box=1.0, device="cuda"):
+    """Forest of independent NFW-like clusters, each centred in its own periodic box
+    [-box/2, box/2)^3: tree sizes n = floor(10^U(log10 lo, log10 hi)), concentration
+    c ~ U(c_range) per tree, radii from the NFW enclosed-mass CDF (bisection),
+    isotropic directions.  Generated with torch on ``device`` (hundreds of millions
+    of points); returns (points (N, 3) float64 tensor, offsets int64 numpy array)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log10(n_range[0]), np.log10(n_range[1])
+    sizes = np.floor(10.0 ** rng.uniform(lo, hi, n_trees)).astype(np.int64)
+    conc = rng.uniform(*c_range, n_trees)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    c = torch.repeat_interleave(torch.from_numpy(conc).to(device),
+                                torch.from_numpy(sizes).to(device))
+    mu = lambda y: torch.log1p(y) - y / (1.0 + y)  # noqa: E731
+    target = torch.rand(c.shape[0], generator=g, device=device, dtype=torch.float64) * mu(c)
+    a = torch.zeros_like(c)
+    b = torch.ones_like(c)
+    for _ in range(40):
+        m = 0.5 * (a + b)
+        below = mu(c * m) < target
+        a = torch.where(below, m, a)
+        b = torch.where(below, b, m)
+    r = 0.5 * (a + b) * rvir * box
+    del a, b, target
+    v = torch.randn((c.shape[0], 3), generator=g, device=device, dtype=torch.float64)
+    v /= torch.linalg.norm(v, dim=1, keepdim=True)
+    pos = torch.remainder(r[:, None] * v + 0.5 * box, box) - 0.5 * box
+    pos[pos >= 0.5 * box] = -0.5 * box
+    return pos.contiguous(), off
