@@ -38,6 +38,8 @@ int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
 static std::atomic<int> g_learned_kernel{0}, g_gather_wpb{2};
 int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); }
 int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
+static std::atomic<int> g_order_mode{0};
+int query_order_mode() { return g_order_mode.load(std::memory_order_relaxed); }
 void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -452,6 +454,10 @@ ckd_status ckd_set_tuning(int key, int value) {
     case 5:
       if (value < 1 || value > 4) return fail(CKD_ERR_BAD_ARG, "gather warps per block must be 1..4");
       g_gather_wpb.store(value);
+      return CKD_OK;
+    case 6:
+      if (value < 0 || value > 2) return fail(CKD_ERR_BAD_ARG, "query ordering must be 0, 1 or 2");
+      g_order_mode.store(value);
       return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");

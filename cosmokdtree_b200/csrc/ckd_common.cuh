@@ -46,6 +46,8 @@ int knn_warps_per_block();
 // warps per block of the gather kernel
 int learned_kernel();
 int gather_warps_per_block();
+// query leaf ordering before a search: 0 automatic, 1 always, 2 never
+int query_order_mode();
 
 // events bracketing the main search kernel when kernel timing is on
 void timing_begin(cudaStream_t s);

@@ -2344,7 +2344,13 @@ ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* 
 }
 
 // Queries are ordered by leaf when there are enough of them to fill many warps.
-bool want_order(const ckd_tree* t, int64_t nq) { return nq >= 4096 && nq * 8 >= t->n / 64; }
+// (tuning key 6: 0 automatic, 1 always, 2 never)
+bool want_order(const ckd_tree* t, int64_t nq) {
+  const int mode = query_order_mode();
+  if (mode == 1) return nq > 1;
+  if (mode == 2) return false;
+  return nq >= 4096 && nq * 8 >= t->n / 64;
+}
 
 ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
                        const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,

@@ -111,7 +111,9 @@ ckd_status ckd_set_knn_variant(int variant);
  * of the kNN kernel (1..8, default 4); key 3: radius factor of the warp-per-bucket
  * kNN search in hundredths (default 150 = 1.5x the density estimate); key 4:
  * search kernel of ckd_knn_learned (0 = bounded per-lane traversal, default;
- * 1 = warp gather); key 5: warps per block of the warp-gather kernel (1..4, default 2). */
+ * 1 = warp gather); key 5: warps per block of the warp-gather kernel (1..4, default 2);
+ * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
+ * default; 1 = always; 2 = never). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference
