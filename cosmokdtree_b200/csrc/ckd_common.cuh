@@ -42,7 +42,8 @@ int knn_variant();
 // tuning knobs (see ckd_set_tuning): blocks-per-SM cap (0 = none), warps per block
 int knn_blocks_per_sm();
 int knn_warps_per_block();
-// learned-bound search kernel: 0 bounded per-lane (k_knn_lane), 1 warp gather;
+// learned-bound search kernel: 0 bounded per-lane with compact heap (k_knn_lane2),
+// 1 warp gather, 2 bounded per-lane with the wide heap (k_knn_lane);
 // warps per block of the gather kernel
 int learned_kernel();
 int gather_warps_per_block();

@@ -831,6 +831,330 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
   }
 }
 
+// ============================================ per-lane traversal, compact heap
+// Same search as k_knn_lane with a heap half the size: each entry is the FP32
+// rounding of its FP64 squared distance (round to nearest is monotone, so
+// a < b in FP32 implies a < b exactly) and the point's leaf-ordered position.
+// Ties in FP32 are resolved exactly by recomputing the FP64 distances from the
+// positions and then comparing ids; the FP64 distances of the results are
+// recomputed once for the output.  8 bytes per entry instead of 12 lets 1.5x
+// more warps stay resident; heap comparisons are 32-bit.  Sentinels: position -1
+// = (HUGE, id -1), position -2 = (r2, INT32_MAX) for the bounded search.
+constexpr int32_t kPosMissing = -1;
+constexpr int32_t kPosBound = -2;
+
+template <int D, bool PER>
+struct CompactCtx {
+  const TreeView& tv;
+  const double (&q)[D];
+  double rr;  // bounded sentinel's squared distance
+  __device__ __forceinline__ double exact(int32_t p) const {
+    return p >= 0 ? point_d2<D, PER>(tv, q, p) : (p == kPosMissing ? CKD_HUGE : rr);
+  }
+  __device__ __forceinline__ int32_t id(int32_t p) const {
+    return p >= 0 ? __ldg(&tv.ids[p]) : (p == kPosMissing ? -1 : 0x7fffffff);
+  }
+  // exact (d2, id) order of two entries whose FP32 keys are equal
+  __device__ __forceinline__ bool tie_before(int32_t a, int32_t b) const {
+    const double da = exact(a), db = exact(b);
+    if (da != db) return da < db;
+    return id(a) < id(b);
+  }
+};
+
+__device__ __forceinline__ float f32_above(float x) {  // next float up (x finite, >= 0)
+  return __uint_as_float(__float_as_uint(x) + 1u);
+}
+
+template <int D, bool PER, bool BOUNDED = false>
+__global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double* __restrict__ Q,
+                                                   const int32_t* __restrict__ order, int64_t nq,
+                                                   int k, int sorted, double* __restrict__ dist,
+                                                   int64_t* __restrict__ idx,
+                                                   unsigned long long* __restrict__ stats,
+                                                   const double* __restrict__ r2 = nullptr,
+                                                   int32_t* __restrict__ miss = nullptr,
+                                                   unsigned* __restrict__ nmiss = nullptr,
+                                                   const int32_t* __restrict__ qleaf = nullptr,
+                                                   const int32_t* __restrict__ qroot = nullptr) {
+  constexpr int NV = (D + 3) / 4;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int KS = heap_stride(k);
+  float* keys = reinterpret_cast<float*>(smem) + (size_t)w * 32 * KS;
+  int32_t* poss = reinterpret_cast<int32_t*>(smem) + (size_t)nw * 32 * KS + (size_t)w * 32 * KS;
+  const int64_t gw = (int64_t)blockIdx.x * nw + w;
+  const int64_t slot = gw * 32 + lane;
+  const bool valid = slot < nq;
+  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  double q[D];
+  QueryScreen<D, PER> qs;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    q[j] = valid ? Q[qi * D + j] : 0.0;
+    qs.q32[j] = __double2float_rn(q[j]);
+    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
+  }
+  float* hk = keys + lane * KS;
+  int32_t* hp = poss + lane * KS;
+  float skey = FLT_MAX;
+  int32_t spos = kPosMissing;
+  float wd32 = FLT_MAX;
+  double rr = CKD_HUGE;
+  if (BOUNDED && valid) {
+    const double b = r2[qi];
+    if (b < CKD_HUGE) {
+      rr = b;
+      skey = __double2float_rn(b);
+      spos = kPosBound;
+      wd32 = __double2float_ru(b);
+    }
+  }
+  const CompactCtx<D, PER> cx{tv, q, rr};
+  for (int s = 1; s <= k; ++s) {
+    hk[s] = skey;
+    hp[s] = spos;
+  }
+  float wk = skey;      // root key
+  int32_t wp = spos;    // root position
+
+  int32_t sn[kLaneStack];
+  float sd[kLaneStack];
+  int top = 0;
+  int32_t node = valid ? (qroot ? qroot[qi] : 0) : -1;
+  if (BOUNDED && valid && qleaf && spos == kPosBound) {
+    // start at the lowest ancestor whose cell strictly contains [q - r, q + r]^D
+    const float r32 = __fsqrt_ru(wd32);
+    int32_t a = qleaf[qi];
+    while (a >= 0) {
+      const float* c = tv.cell32 + (int64_t)a * 2 * D;
+      bool inside = true;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        const float2 lh = __ldg(reinterpret_cast<const float2*>(c) + j);
+        inside = inside && __fsub_rd(__fsub_rd(qs.q32[j], r32), qs.dlt[j]) > lh.x &&
+                 __fadd_ru(__fadd_ru(qs.q32[j], r32), qs.dlt[j]) < lh.y;
+      }
+      if (inside) break;
+      a = load_meta(tv.meta, a).parent;
+    }
+    node = a < 0 ? node : a;
+  }
+  while (node >= 0) {
+    // ---- descend to a leaf, nearer child first
+    NodeMeta m = load_meta(tv.meta, node);
+    while (node >= 0 && m.left >= 0) {
+      if (stats) st[0] += 1;
+      float ml = node_mind_lb<D, PER>(tv, qs, m.left);
+      float mr = node_mind_lb<D, PER>(tv, qs, m.left + 1);
+      bool nl = ml <= wd32, nr = mr <= wd32;
+      if (nl && nr) {
+        bool lf = ml <= mr;
+        sn[top] = lf ? m.left + 1 : m.left;
+        sd[top] = lf ? mr : ml;
+        ++top;
+        node = lf ? m.left : m.left + 1;
+      } else if (nl || nr) {
+        node = nl ? m.left : m.left + 1;
+      } else {
+        node = -1;
+        while (top > 0) {
+          --top;
+          if (sd[top] <= wd32) {
+            node = sn[top];
+            break;
+          }
+        }
+      }
+      if (node >= 0) m = load_meta(tv.meta, node);
+    }
+    if (node < 0) break;
+    // ---- scan the leaf
+    if (stats) {
+      st[2] += 1;
+      st[3] += m.count;
+    }
+    float qr[D], e[D];
+    {
+      const double* b = tv.box + (int64_t)node * 2 * D;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        double lo = __ldg(&b[2 * j]), hh = __ldg(&b[2 * j + 1]);
+        double c = leaf_centre(lo, hh);
+        double r = fmax(c - lo, hh - c);
+        double x = q[j] - c;
+        if (PER) {
+          double h = 0.5 * tv.L[j];
+          if (x > h) x -= tv.L[j];
+          else if (x < -h) x += tv.L[j];
+        }
+        qr[j] = __double2float_rn(x);
+        e[j] = kTwoM21 * (float)(r + fabs(x) + (PER ? tv.L[j] : 0.0)) * 1.0001f + 1e-37f;
+      }
+    }
+    for (int base = 0; base < m.count; base += 32) {
+      const int cnt = min(32, m.count - base);
+      const int32_t p0 = m.start + base;
+      unsigned mask = 0;
+      for (int i = 0; i < cnt; ++i) {
+        float v[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+          v[4 * h] = f.x;
+          v[4 * h + 1] = f.y;
+          v[4 * h + 2] = f.z;
+          v[4 * h + 3] = f.w;
+        }
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float a = fabsf(v[j] - qr[j]);
+          if (PER) a = fminf(a, (float)tv.L[j] - a);
+          a = fmaxf(a - e[j], 0.0f);
+          s = fmaf(a, a, s);
+        }
+        if (s * kShrink <= wd32) mask |= 1u << i;
+      }
+      if (stats) st[5] += __popc(mask);
+      while (mask) {
+        const int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const int32_t p = p0 + i;
+        const double d2 = point_d2<D, PER>(tv, q, p);
+        const float kc = __double2float_rn(d2);
+        if (kc > wk) continue;
+        if (kc == wk) {  // FP32 tie with the root: exact comparison
+          const double dr = cx.exact(wp);
+          if (d2 > dr) continue;
+          if (d2 == dr && __ldg(&tv.ids[p]) >= cx.id(wp)) continue;
+        }
+        if (stats) st[6] += 1;
+        // replace the root, sift down
+        int s = 1;
+        for (;;) {
+          const int l = 2 * s;
+          if (l > k) break;
+          float kch;
+          int32_t pch;
+          int c;
+          if (l < k) {
+            const float2 kk = *reinterpret_cast<const float2*>(hk + l);
+            const int2 pp = *reinterpret_cast<const int2*>(hp + l);
+            const bool right = kk.x < kk.y || (kk.x == kk.y && cx.tie_before(pp.x, pp.y));
+            kch = right ? kk.y : kk.x;
+            pch = right ? pp.y : pp.x;
+            c = right ? l + 1 : l;
+          } else {
+            kch = hk[l];
+            pch = hp[l];
+            c = l;
+          }
+          // the candidate stays above the child iff it ranks after it
+          bool cand_before = kc < kch;
+          if (kc == kch) {
+            const double dch = cx.exact(pch);
+            cand_before = d2 < dch || (d2 == dch && __ldg(&tv.ids[p]) < cx.id(pch));
+          }
+          if (!cand_before) break;
+          hk[s] = kch;
+          hp[s] = pch;
+          s = c;
+        }
+        hk[s] = kc;
+        hp[s] = p;
+        wk = hk[1];
+        wp = hp[1];
+        wd32 = f32_above(wk);
+      }
+    }
+    // ---- next: pop the nearest pending subtree still within reach
+    node = -1;
+    while (top > 0) {
+      --top;
+      if (sd[top] <= wd32) {
+        node = sn[top];
+        break;
+      }
+    }
+  }
+  if (stats) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      unsigned long long v = st[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+      if (lane == 0) atomicAdd(&stats[c], v);
+    }
+  }
+  const bool missed = BOUNDED && valid && wp == kPosBound;
+  unsigned missmask = 0;
+  if (BOUNDED) {
+    missmask = __ballot_sync(FULL, missed);
+    if (missmask) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(nmiss, (unsigned)__popc(missmask));
+      base = __shfl_sync(FULL, base, 0);
+      if (missed) miss[base + __popc(missmask & ((1u << lane) - 1u))] = (int32_t)qi;
+    }
+  }
+  if (sorted && valid && !missed) {
+    for (int end = k; end > 1; --end) {
+      const float key = hk[end];
+      const int32_t pk = hp[end];
+      hk[end] = hk[1];
+      hp[end] = hp[1];
+      int s = 1;
+      for (;;) {
+        const int l = 2 * s;
+        if (l >= end) break;
+        int c = l;
+        float kc = hk[l];
+        int32_t pc = hp[l];
+        if (l + 1 < end) {
+          const float kr = hk[l + 1];
+          const int32_t pr = hp[l + 1];
+          if (kc < kr || (kc == kr && cx.tie_before(pc, pr))) {
+            c = l + 1;
+            kc = kr;
+            pc = pr;
+          }
+        }
+        if (!(key < kc || (key == kc && cx.tie_before(pk, pc)))) break;
+        hk[s] = kc;
+        hp[s] = pc;
+        s = c;
+      }
+      hk[s] = key;
+      hp[s] = pk;
+    }
+  }
+  __syncwarp();
+  // warp-cooperative write-out: exact FP64 distances recomputed from positions
+  for (int qq = 0; qq < 32; ++qq) {
+    const int64_t s2 = gw * 32 + qq;
+    if (s2 >= nq) break;
+    double qx[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) qx[j] = __shfl_sync(FULL, q[j], qq);
+    if (BOUNDED && ((missmask >> qq) & 1u)) continue;
+    const int64_t row = order ? (int64_t)order[s2] : s2;
+    const int32_t* rp = poss + qq * KS + 1;
+    for (int j = lane; j < k; j += 32) {
+      const int32_t p = rp[j];
+      double d2 = CKD_HUGE;
+      int64_t id = -2;
+      if (p >= 0) {
+        d2 = point_d2<D, PER>(tv, qx, p);
+        id = (int64_t)__ldg(&tv.ids[p]);
+      }
+      dist[row * k + j] = sqrt(d2);
+      idx[row * k + j] = id;
+    }
+  }
+}
+
 // ===================================================== bottom-up search (v4)
 // Per-lane search that starts at the query's own leaf and climbs: after a
 // subtree C is exhausted, the search stops if the ball of the current k-th
@@ -2192,7 +2516,21 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
   bool use_gstack = stack_len > kStack || k > kSmemK;
   if (use_gstack)
     CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
-  if (k <= kSmemK && t->screen_ok && (var == 0 || var == 3) && t->depth < kLaneStack - 1) {
+  if (k <= kSmemK && t->screen_ok && (var == 0 || var == 7) && t->depth < kLaneStack - 1) {
+    const int nw7 = std::min(4, knn_warps_per_block());
+    const unsigned blocks7 = (unsigned)cdiv(cdiv(nq, 32), nw7);
+    size_t sm = (size_t)nw7 * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    const int bps = knn_blocks_per_sm();
+    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm));
+    k_knn_lane2<D, PER><<<blocks7, nw7 * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
+                                                      knn_stats_buffer());
+    CKD_LAUNCH_CHECK();
+    if (gstack) CKD_CUDA(dev_free(gstack, s));
+    return CKD_OK;
+  }
+  if (k <= kSmemK && t->screen_ok && var == 3 && t->depth < kLaneStack - 1) {
     size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
     CKD_CUDA(cudaFuncSetAttribute(k_knn_lane<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm));
@@ -2301,7 +2639,7 @@ ckd_status bucket_run(const ckd_tree* t, const double* q, int64_t nq, int k, dou
   CKD_CUDA(cudaStreamSynchronize(s));
   if ((int64_t)nfallback > nq) return fail(CKD_ERR_CUDA, "internal error: fallback list overflow");
   ckd_status st = CKD_OK;
-  if (nfallback > 0) st = knn_launch<D, PER>(t, q, fb, nullptr, nfallback, k, 1, dist, idx, s, 3);
+  if (nfallback > 0) st = knn_launch<D, PER>(t, q, fb, nullptr, nfallback, k, 1, dist, idx, s, 7);
   for (void* p : {(void*)order, (void*)off, (void*)nb, (void*)nbo, (void*)fb, (void*)nfb,
                   (void*)buckets})
     dev_free(p, s);
@@ -2415,21 +2753,21 @@ ckd_status forest_knn_impl(const ckd_tree* t, const double* q, const int32_t* qr
   CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
   ckd_status st = order_impl<D>(t, q, nq, order, nullptr, s, nullptr, qroot);
   if (st == CKD_OK) {
-    const int nw = knn_warps_per_block();
+    const int nw = std::min(4, knn_warps_per_block());
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
-    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
-    cudaError_t e = cudaFuncSetAttribute(k_knn_lane<D, PER>,
+    cudaError_t e = cudaFuncSetAttribute(k_knn_lane2<D, PER>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) {
       dev_free(order, s);
-      return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane)");
+      return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane2)");
     }
     timing_begin(s);
-    k_knn_lane<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist, idx,
-                                                   knn_stats_buffer(), nullptr, nullptr, nullptr,
-                                                   nullptr, qroot);
+    k_knn_lane2<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist, idx,
+                                                    knn_stats_buffer(), nullptr, nullptr, nullptr,
+                                                    nullptr, qroot);
     note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) st = cuda_fail(e, "k_knn_lane (forest)");
@@ -2486,6 +2824,21 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     st = mlp_radius(t, net, q, order, qleaf, nq, k, r2, s);
   }
   if (st == CKD_OK && learned_kernel() == 0) {
+    const int nw = std::min(4, knn_warps_per_block());
+    const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    const int bps = knn_blocks_per_sm();
+    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
+    cudaError_t e = cudaFuncSetAttribute(k_knn_lane2<D, PER, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane2)");
+    k_knn_lane2<D, PER, true><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted,
+                                                          dist, idx, knn_stats_buffer(), r2, miss,
+                                                          nmiss, qleaf);
+    note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) st = cuda_fail(e, "k_knn_lane2 (bounded)");
+  } else if (st == CKD_OK && learned_kernel() == 2) {
     const int nw = knn_warps_per_block();
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
     size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
@@ -2521,7 +2874,7 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     else if ((int64_t)nm > nq) st = fail(CKD_ERR_CUDA, "internal error: fallback list overflow");
   }
   if (st == CKD_OK && nm > 0)
-    st = knn_launch<D, PER>(t, q, miss, nullptr, (int64_t)nm, k, sorted, dist, idx, s, 3);
+    st = knn_launch<D, PER>(t, q, miss, nullptr, (int64_t)nm, k, sorted, dist, idx, s, 7);
   if (st == CKD_OK) timing_end(s);
   if (nfb_out) *nfb_out = nm;
   for (void* p : {(void*)order, (void*)qleaf, (void*)r2, (void*)miss, (void*)nmiss}) dev_free(p, s);
@@ -2658,10 +3011,11 @@ ckd_status knn_noalloc_impl(const ckd_tree* t, const double* q, int64_t nq, int 
   const int nw = 4;
   const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
   if (t->screen_ok && t->depth < kLaneStack - 1) {
-    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(unsigned long long) + sizeof(int32_t));
-    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm));
-    k_knn_lane<D, PER><<<blocks, nw * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx, nullptr);
+    k_knn_lane2<D, PER><<<blocks, nw * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
+                                                    nullptr);
   } else {
     size_t sm = (size_t)nw * k * 32 * (sizeof(double) + sizeof(int32_t)) +
                 (size_t)nw * kStack * sizeof(int32_t);

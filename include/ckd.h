@@ -96,22 +96,24 @@ ckd_status ckd_knn_ordered(const ckd_tree* tree, const double* q_dev, int64_t nq
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t ckd_launch_count(void);
 
-/* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (the
- * per-lane FP32-screened traversal when k <= 64, the coordinates allow the FP32
- * screen and the tree is shallow enough, else 2), 1 = FP64-only packet
- * traversal, 2 = FP32-screened packet traversal, 3 = per-lane traversal,
- * 4 = bottom-up per-lane search, 5 = persistent per-lane search, 6 = warp per
- * bucket with a density radius.  Every variant returns the same exact result. */
+/* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (7
+ * when k <= 64, the coordinates allow the FP32 screen and the tree is shallow
+ * enough, else 2), 1 = FP64-only packet traversal, 2 = FP32-screened packet
+ * traversal, 3 = per-lane traversal with 12-byte heap entries, 4 = bottom-up
+ * per-lane search, 5 = persistent per-lane search, 6 = warp per bucket with a
+ * density radius, 7 = per-lane traversal with 8-byte heap entries (FP32 key +
+ * position, exact tie resolution).  Every variant returns the same exact result. */
 ckd_status ckd_set_knn_variant(int variant);
 
 /* Process-wide launch tuning of the search kernels (no reference counterpart;
  * set by the autotuner).  key 0: kNN variant (as ckd_set_knn_variant);
  * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
  * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
- * of the kNN kernel (1..8, default 4); key 3: radius factor of the warp-per-bucket
+ * of the kNN kernel (1..8, default 2; the per-lane kernels use at most 4); key 3: radius factor of the warp-per-bucket
  * kNN search in hundredths (default 150 = 1.5x the density estimate); key 4:
- * search kernel of ckd_knn_learned (0 = bounded per-lane traversal, default;
- * 1 = warp gather); key 5: warps per block of the warp-gather kernel (1..4, default 2);
+ * search kernel of ckd_knn_learned (0 = bounded per-lane traversal with 8-byte
+ * heap entries, default; 1 = warp gather; 2 = bounded per-lane with 12-byte
+ * entries); key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
  * default; 1 = always; 2 = never). */
 ckd_status ckd_set_tuning(int key, int value);

@@ -83,9 +83,17 @@ def test_features_match_numpy(gpu):
     np.testing.assert_allclose(f, ref, rtol=0, atol=2e-4)
 
 
+@pytest.fixture(params=[0, 1, 2], ids=["bounded_lane_compact", "gather", "bounded_lane_wide"])
+def learned_kernel(request, gpu):
+    from cosmokdtree_b200 import _lib
+    _lib.check(_lib.load().ckd_set_tuning(4, request.param))
+    yield request.param
+    _lib.load().ckd_set_tuning(4, 0)
+
+
 @pytest.mark.parametrize("k", [8, 32])
 @pytest.mark.parametrize("margin_shift", [-1.0, 0.0, 3.0])
-def test_learned_knn_is_exact(trained, k, margin_shift):
+def test_learned_knn_is_exact(trained, learned_kernel, k, margin_shift):
     from cosmokdtree_b200 import kdtree
     t, P, lb, info = trained
     rng = np.random.default_rng(46)
@@ -150,7 +158,7 @@ def test_learned_bound_saves_work(trained):
         _lib.check(L.ckd_knn_stats(0, out))
         return np.array(out[:])
 
-    _lib.check(L.ckd_set_knn_variant(3))
+    _lib.check(L.ckd_set_knn_variant(7))
     try:
         plain = stats(lambda: kdtree.knn_search(t, Q, 32))
         learned = stats(lambda: lb.knn(t, Q, 32))

@@ -68,6 +68,8 @@ def make_points(name, n, d, periodic, seed=0):
     rng = np.random.default_rng(seed + hash(name) % 1000)
     if "clustered" in name:
         P = clustered(rng, n, d, periodic, dup=200 if "dup" in name else 0)
+    elif "lattice" in name:  # many exactly equal distances (ties broken by id)
+        P = rng.integers(-8, 8, (n, d)).astype(np.float64) / 16.0
     else:
         P = rng.random((n, d)) - (0.5 if periodic else 0.0)
     return P
@@ -105,11 +107,14 @@ KNN_CASES = [
     ("d6", 30000, 6, False, 32, 3000, 64),
     ("d2", 20000, 2, True, 4, 3000, 7),
     ("uniform3d", 20000, 3, False, 16, 500, 100),
+    ("lattice", 30000, 3, False, 16, 3000, 24),
+    ("lattice_periodic", 30000, 3, True, 16, 3000, 40),
 ]
 
 
-@pytest.fixture(params=[1, 2, 3, 4, 5, 6],
-                ids=["fp64", "screened", "lane", "bottom_up", "persistent", "bucket"])
+@pytest.fixture(params=[1, 2, 3, 4, 5, 6, 7],
+                ids=["fp64", "screened", "lane", "bottom_up", "persistent", "bucket",
+                     "lane_compact"])
 def knn_variant(request, gpu):
     from cosmokdtree_b200 import _lib
     _lib.check(_lib.load().ckd_set_knn_variant(request.param))
