@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark: exact kNN queries/s (k=32, self-query) over a 16.7M-point clustered
-periodic catalogue on one B200 -- learned-bound search (headline ``value``) and the
-plain search (``plain``), both exact and checked equal -- plus build Mpt/s.
+periodic catalogue on one B200 -- the default search (headline ``value``) and the
+learned-bound search (``learned``, with its ratio), both exact and checked equal --
+plus build Mpt/s and ball search (r = half the mean spacing, CSR).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -43,6 +44,23 @@ WORKLOADS = {
     "clustered_periodic_2p22_k32": (1 << 22, 32, True, 16, 1),
 }
 DEFAULT_WORKLOAD = "clustered_periodic_2p24_k32"
+# learned-bound configurations with their own query sets (several k, other dims)
+MULTI_WORKLOADS = {
+    # 2^26 clustered periodic, 10^7 queries (half particles, half uniform), k in {8,32,64}
+    "learned_mixed_2p26": dict(n=1 << 26, d=3, periodic=True, leaf=16, ks=(8, 32, 64),
+                               nq=10_000_000, query="mixed", dtype="f64", seed=1,
+                               train_seed=3, query_seed=4),
+    "learned_mixed_2p22": dict(n=1 << 22, d=3, periodic=True, leaf=16, ks=(8, 32, 64),
+                               nq=1_000_000, query="mixed", dtype="f64", seed=1,
+                               train_seed=3, query_seed=4),
+    # 2^27 6-D phase space, float32 input, leaf 32, 2x10^7 queries, k = 64
+    "phase6d_2p27_k64": dict(n=1 << 27, d=6, periodic=False, leaf=32, ks=(64,),
+                             nq=20_000_000, query="particles", dtype="f32", seed=5,
+                             train_seed=6, query_seed=7),
+    "phase6d_2p22_k64": dict(n=1 << 22, d=6, periodic=False, leaf=32, ks=(64,),
+                             nq=1_000_000, query="particles", dtype="f32", seed=5,
+                             train_seed=6, query_seed=7),
+}
 # forests: name -> (n_trees, k, boxes per tree, box side, seed)
 FOREST_WORKLOADS = {
     "forest_2000_nfw_k8": (2000, 8, 64, 0.05, 2),
@@ -308,6 +326,156 @@ def run_forest(args):
     return 0
 
 
+def run_multi(args):
+    """Learned-bound vs plain kNN on a configuration with its own queries: several k
+    (queries split evenly, one search call per k), optional 6-D float32 input.  The
+    network is trained on 10^6 exact k-th distances of a separate catalogue of the
+    same size and kind (train_seed) with queries drawn the same way."""
+    import torch
+    from cosmokdtree_b200 import _lib, kdtree, synth
+    from cosmokdtree_b200.learned import LearnedBound
+    cfg = MULTI_WORKLOADS[args.workload]
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L = _lib.load()
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    n, d, ks, nq = cfg["n"], cfg["d"], cfg["ks"], cfg["nq"]
+    box = [1.0] * d if cfg["periodic"] else None
+
+    def catalogue(seed):
+        if d == 6:
+            return synth.phase_space(n, seed=seed, dtype=np.float32 if cfg["dtype"] == "f32"
+                                     else np.float64)
+        return synth.clustered_periodic(n, seed=seed)
+
+    def queries(P, seed, m):
+        if cfg["query"] == "mixed":
+            return synth.mixed_queries(P, m, seed)
+        rng = np.random.default_rng(seed)
+        return np.ascontiguousarray(P[rng.integers(0, P.shape[0], m)].astype(np.float64))
+
+    t0 = time.perf_counter()
+    P = catalogue(cfg["seed"])
+    gen_s = time.perf_counter() - t0
+    Pd = torch.from_numpy(P).cuda()
+    build_ms = []
+    for it in range(2):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tree = kdtree.build_kdtree(Pd, leaf=cfg["leaf"], boxsize=box)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        build_ms.append(e0.elapsed_time(e1))
+        if it == 0:
+            tree.close()
+    del Pd
+    # training on a separate catalogue
+    t0 = time.perf_counter()
+    Ptr = catalogue(cfg["train_seed"])
+    ttr = kdtree.build_kdtree(torch.from_numpy(Ptr).cuda(), leaf=cfg["leaf"], boxsize=box)
+    Qtr = torch.from_numpy(queries(Ptr, cfg["train_seed"] + 100, 1_000_000)).cuda()
+    lb = LearnedBound(seed=0)
+    fit = lb.fit(ttr, Qtr, list(ks), epochs=30, batch=4096, lr=3e-3, quantile=0.97)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    ttr.close()
+    del Ptr, Qtr
+    # evaluation queries, split evenly over the k values
+    Qh = queries(P, cfg["query_seed"], nq)
+    kq = np.random.default_rng(cfg["query_seed"] + 1).integers(0, len(ks), nq)
+    groups = []
+    for gi, k in enumerate(ks):
+        qg = torch.from_numpy(np.ascontiguousarray(Qh[kq == gi])).cuda()
+        m = qg.shape[0]
+        outs = [(torch.empty((m, k), dtype=torch.float64, device="cuda"),
+                 torch.empty((m, k), dtype=torch.int64, device="cuda")) for _ in range(2)]
+        groups.append((k, qg, outs))
+    nfb = ctypes.c_int64()
+    fallbacks = {}
+
+    def plain_step():
+        for k, qg, outs in groups:
+            _lib.check(L.ckd_knn(tree.handle, ctypes.c_void_p(qg.data_ptr()), qg.shape[0], k, 1,
+                                 ctypes.c_void_p(outs[0][0].data_ptr()),
+                                 ctypes.c_void_p(outs[0][1].data_ptr()), sp))
+
+    def learned_step():
+        for k, qg, outs in groups:
+            _lib.check(L.ckd_knn_learned(tree.handle, lb.handle, ctypes.c_void_p(qg.data_ptr()),
+                                         qg.shape[0], k, 1,
+                                         ctypes.c_void_p(outs[1][0].data_ptr()),
+                                         ctypes.c_void_p(outs[1][1].data_ptr()),
+                                         ctypes.byref(nfb), sp))
+            fallbacks[k] = int(nfb.value)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    l0 = L.ckd_launch_count()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        plain_ms = timed(plain_step)
+        learned_ms = timed(learned_step)
+    launches = (L.ckd_launch_count() - l0) // (2 * (args.steps + args.warmup))
+    exact = all(torch.equal(o[0][0], o[1][0]) and torch.equal(o[0][1], o[1][1])
+                for _, _, o in groups)
+    # oracle parity on a sample and CPU baseline
+    import oracle
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ot = oracle.OracleTree(P.astype(np.float64), cfg["leaf"], box, threads=threads)
+    cpu_build_s = time.perf_counter() - t0
+    parity = True
+    cpu_q, cpu_s = 0, 0.0
+    for k, qg, outs in groups:
+        qs = qg[:2000].cpu().numpy()
+        t1 = time.perf_counter()
+        od, oi = ot.knn(qs, k)
+        cpu_s += time.perf_counter() - t1
+        cpu_q += len(qs)
+        parity = parity and np.array_equal(oi, outs[1][1][:2000].cpu().numpy()) and \
+            np.array_equal(od, outs[1][0][:2000].cpu().numpy())
+    ot.close()
+    out = {
+        "metric": "knn_queries_per_s", "value": nq / (learned_ms / 1e3), "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n_points": n, "dims": d, "n_queries": nq,
+                   "k": list(ks), "queries": cfg["query"], "input_dtype": cfg["dtype"],
+                   "leaf": cfg["leaf"], "periodic": cfg["periodic"], "seed": cfg["seed"],
+                   "l2": "inputs larger than L2"},
+        "plain": {"value": nq / (plain_ms / 1e3), "ms_per_step": plain_ms},
+        "learned": {"value": nq / (learned_ms / 1e3), "speedup_vs_plain": plain_ms / learned_ms,
+                    "exact_vs_plain": bool(exact),
+                    "fallback_rate": {str(k): fallbacks[k] / max(1, g[1].shape[0])
+                                      for k, g in zip(ks, groups)},
+                    "train_s": train_s, "margin_log2": fit["margin"],
+                    "holdout_rms_log2": fit["holdout_rms_log2"]},
+        "cpu_baseline": {"value": cpu_q / cpu_s, "unit": "queries/s", "cores": threads,
+                         "kind": "port", "sample": f"{cpu_q} queries (2000 per k), FP64"},
+        "gpu_launches_per_step": int(launches),
+        "clocks": clk.summary(),
+        "build": {"ms": build_ms[-1], "mpts_per_s": n / (build_ms[-1] / 1e3) / 1e6,
+                  "cpu_s": cpu_build_s, "depth": tree.depth},
+        "parity_sample": {"rows": cpu_q, "bit_exact": bool(parity)},
+        "generation_s": gen_s,
+    }
+    print(json.dumps(out))
+    tree.close()
+    lb.close()
+    return 0
+
+
 def workload_config(name):
     n, k, periodic, leaf, seed = WORKLOADS[name]
     return {"workload": name, "n_points": n, "n_queries": n, "k": k, "sorted": True,
@@ -322,7 +490,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(WORKLOADS) + sorted(FOREST_WORKLOADS))
+                    choices=sorted(WORKLOADS) + sorted(FOREST_WORKLOADS) +
+                    sorted(MULTI_WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -333,13 +502,15 @@ def main():
                     help="one build and the kNN steps only (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
-        if args.workload in FOREST_WORKLOADS:
-            print(json.dumps({"impl": "reference", "unavailable": "the forest workload's CPU "
-                              "baseline is reported inside the ours line (sampled trees)"}))
+        if args.workload in FOREST_WORKLOADS or args.workload in MULTI_WORKLOADS:
+            print(json.dumps({"impl": "reference", "unavailable": "this workload's CPU "
+                              "baseline is reported inside the ours line (sampled queries)"}))
             return 0
         return run_reference(args)
     if args.workload in FOREST_WORKLOADS:
         return run_forest(args)
+    if args.workload in MULTI_WORKLOADS:
+        return run_multi(args)
 
     import torch
     import torch.distributed as dist
@@ -481,9 +652,51 @@ def main():
     exact = bool(torch.equal(idx_l, idx_t) and torch.equal(dist_l, dist_t))
     exact = allmax(0.0 if exact else 1.0) == 0.0
     plain_value = world * nq * args.steps / (plain_total / 1e3)
-    value = world * nq * args.steps / (learned_total / 1e3)
-    ms_per_step = learned_total / args.steps
+    learned_value = world * nq * args.steps / (learned_total / 1e3)
+    # headline: the default exact path (knn_search / ckd_knn); the learned-bound
+    # search is reported beside it with its ratio
+    value = plain_value
+    ms_per_step = plain_total / args.steps
     clocks = clk.summary()
+
+    # ---- ball search over the same queries: r = half the mean interparticle spacing.
+    # Inside the NFW cusps a query holds up to ~10^5 neighbours within r, so the
+    # full result (about 10^12 ids) cannot be materialised: the count pass (phase 1
+    # of the CSR protocol) runs over every query, the full count + scan + fill over
+    # a random subset whose CSR fits in 2 GB.
+    radius = 0.5 * n ** (-1.0 / 3.0)
+    counts = torch.empty(nq, dtype=torch.int64, device="cuda")
+    cp = ctypes.c_void_p(counts.data_ptr())
+
+    def ball_count_step():
+        _lib.check(L.ckd_ball_count(tree.handle, qp, nq, radius, cp, sp))
+
+    ball_count_total, _, _ = timed(ball_count_step, args.steps, args.warmup)
+    total_hits = int(counts.sum().item())
+    mean_hits = total_hits / nq
+    m_ball = int(min(nq, max(1024, 1.2e8 / max(mean_hits, 1.0))))
+    bq = Q[torch.randperm(nq, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))[:m_ball]].contiguous()
+    bqp = ctypes.c_void_p(bq.data_ptr())
+    bcounts = torch.empty(m_ball, dtype=torch.int64, device="cuda")
+    boff = torch.zeros(m_ball + 1, dtype=torch.int64, device="cuda")
+    _lib.check(L.ckd_ball_count(tree.handle, bqp, m_ball, radius, ctypes.c_void_p(bcounts.data_ptr()), sp))
+    _lib.check(L.ckd_exclusive_scan(ctypes.c_void_p(bcounts.data_ptr()),
+                                    ctypes.c_void_p(boff.data_ptr()), m_ball, sp))
+    n_hits = int(boff[-1].item())
+    bidx = torch.empty(max(1, n_hits), dtype=torch.int64, device="cuda")
+    bdist = torch.empty(max(1, n_hits), dtype=torch.float64, device="cuda")
+
+    def ball_step():
+        _lib.check(L.ckd_ball_count(tree.handle, bqp, m_ball, radius,
+                                    ctypes.c_void_p(bcounts.data_ptr()), sp))
+        _lib.check(L.ckd_exclusive_scan(ctypes.c_void_p(bcounts.data_ptr()),
+                                        ctypes.c_void_p(boff.data_ptr()), m_ball, sp))
+        _lib.check(L.ckd_ball_fill(tree.handle, bqp, m_ball, radius, 0,
+                                   ctypes.c_void_p(boff.data_ptr()),
+                                   ctypes.c_void_p(bidx.data_ptr()),
+                                   ctypes.c_void_p(bdist.data_ptr()), sp))
+
+    ball_total, _, ball_launches = timed(ball_step, args.steps, args.warmup)
     stats = None
     if args.stats:
         names = ["node_tests", "gathered_leaves", "leaf_scans", "points_screened", "flushes",
@@ -504,7 +717,9 @@ def main():
     # ---- end to end through the public API with host buffers (learned and plain)
     def e2e(fn):
         vals = []
+        res = None
         for it in range(args.e2e_steps + 1):
+            res = None  # return the previous result's pinned host buffers to the cache
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -516,8 +731,13 @@ def main():
                 vals.append(e0.elapsed_time(e1))
         return allmax(float(np.mean(vals))), res
 
-    e2e_ms_v, (hd, hi) = e2e(lambda: lb.knn(tree, P, k, sorted=True))
-    e2e_plain_ms, _ = e2e(lambda: kdtree.knn_search(tree, P, k, sorted=True))
+    samp = np.random.default_rng(7).integers(0, nq, 20000)  # parity rows
+    e2e_learned_ms, res = e2e(lambda: lb.knn(tree, P, k, sorted=True))
+    hd, hi = res[0][samp], res[1][samp]
+    del res
+    e2e_ms_v, res = e2e(lambda: kdtree.knn_search(tree, P, k, sorted=True))
+    hd0, hi0 = res[0][samp], res[1][samp]
+    del res
 
     if rank == 0:
         import oracle
@@ -527,10 +747,12 @@ def main():
         t0 = time.perf_counter()
         otree = oracle.OracleTree(P, leaf, 1.0 if periodic else None, threads=threads)
         cpu_build_s = time.perf_counter() - t0
-        rng = np.random.default_rng(7)
-        samp = rng.integers(0, nq, 20000)
         od, oi = otree.knn(P[samp], k)
-        parity = bool(np.array_equal(oi, hi[samp]) and np.array_equal(od, hd[samp]))
+        parity = bool(np.array_equal(oi, hi) and np.array_equal(od, hd) and
+                      np.array_equal(oi, hi0) and np.array_equal(od, hd0))
+        # ball parity on a sample: the count pass against the oracle's CSR
+        bo_o, _, _ = otree.ball_csr(P[samp[:5000]], radius)
+        ball_parity = bool(np.array_equal(np.diff(bo_o), counts[torch.from_numpy(samp[:5000]).cuda()].cpu().numpy()))
         ab = otree.knn_algbytes(P[samp], k, od[:, -1] ** 2)
         bytes_per_q = ab["bytes"] / len(samp)
 
@@ -552,31 +774,46 @@ def main():
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(name),
-            "roofline": roof(learned_kernel_ms, "k_mlp_radius + k_knn_lane (bounded) + rerun"),
+            "roofline": roof(plain_kernel_ms, "k_knn_lane2"),
             "cpu_baseline": cpu,
             "e2e": {"value": world * nq / (e2e_ms_v / 1e3), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * 3 * 8, "d2h_bytes_per_step": nq * k * 16,
                     "ms_per_step": e2e_ms_v},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(plain_launches),
             "clocks": clocks,
             "learned": {"method": "learned-bound kNN (MLP 12-64-64-1, BF16 weights)",
-                        "value": value, "speedup_vs_plain": value / plain_value,
+                        "value": learned_value, "speedup_vs_plain": learned_value / plain_value,
+                        "ms_per_step": learned_total / args.steps,
                         "exact_vs_plain": exact, "fallback_queries": fallback,
                         "fallback_rate": fallback / nq, "kernel_ms": learned_kernel_ms,
+                        "gpu_launches": int(launches),
+                        "roofline": roof(learned_kernel_ms,
+                                         "k_mlp_radius + k_knn_lane2 (bounded) + rerun"),
+                        "e2e_queries_per_s": world * nq / (e2e_learned_ms / 1e3),
                         "train_s": train_s, "train_samples": fit["n_train"],
                         "train_catalogue_seed_offset": 2, "margin_log2": fit["margin"],
                         "holdout_rms_log2": fit["holdout_rms_log2"],
                         "holdout_rerun_rate": fit["holdout_rerun_rate"],
                         "final_loss": fit["loss"][-1]},
             "plain": {"value": plain_value, "ms_per_step": plain_total / args.steps,
-                      "kernel_ms": plain_kernel_ms, "gpu_launches": int(plain_launches),
-                      "roofline": roof(plain_kernel_ms, "k_knn_lane"),
-                      "e2e_queries_per_s": world * nq / (e2e_plain_ms / 1e3)},
+                      "kernel_ms": plain_kernel_ms, "method": "knn_search / ckd_knn (default)"},
+            "ball": {"radius": radius, "unit": "queries/s",
+                     "count_pass": {"queries": nq, "value": world * nq * args.steps /
+                                    (ball_count_total / 1e3),
+                                    "ms_per_step": ball_count_total / args.steps,
+                                    "total_hits": total_hits, "mean_hits": mean_hits},
+                     "count_scan_fill": {"queries": m_ball, "value": world * m_ball * args.steps /
+                                         (ball_total / 1e3),
+                                         "ms_per_step": ball_total / args.steps, "hits": n_hits,
+                                         "output": "CSR, unsorted (reference default)",
+                                         "gpu_launches": int(ball_launches)},
+                     "count_parity_sample": ball_parity},
             "build": {"ms": build_ms_v, "mpts_per_s": n / (build_ms_v / 1e3) / 1e6,
                       "cpu_s": cpu_build_s, "cpu_mpts_per_s": n / cpu_build_s / 1e6,
                       "n_nodes": tree.n_nodes, "depth": tree.depth},
             "breakdown_ms": {"learned_step": float(np.mean(learned_steps)),
-                             "plain_step": float(np.mean(plain_steps))},
+                             "plain_step": float(np.mean(plain_steps)),
+                             "plain_search_kernel": plain_kernel_ms},
             "parity_sample": {"rows": int(len(samp)), "bit_exact": parity},
         }
         if stats:

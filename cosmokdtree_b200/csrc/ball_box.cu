@@ -5,7 +5,8 @@
 // reference's "fully inside" shortcut (:1116-1118, :1332-1366) selects exactly
 // the same points, because a node's max-distance bound is never below the
 // computed distance of a point inside it; the count pass uses it (with the
-// tight box) to skip distance work.  Traversal is left child first, so the
+// tight box) to skip distance work, on periodic trees too when the box lies
+// within half a box side of the query on every axis (box_maxd2_near).  Traversal is left child first, so the
 // unsorted order of a row is the reference's non-periodic order (left-first DFS,
 // leaf order).  sorted=1 orders each row by (d2, id).
 //
@@ -58,7 +59,8 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
     NodeMeta m = load_meta(tv.meta, node);
     bool need = box_mind2<D, PER>(tv, q, node) <= rr;
     if (!FILL && need && m.start >= cov_lo && m.start < cov_hi) need = false;
-    if (!FILL && !PER && need && m.left >= 0 && box_maxd2<D>(tv, q, node) <= rr) {
+    if (!FILL && need && m.left >= 0 &&
+        (PER ? box_maxd2_near<D>(tv, q, node) : box_maxd2<D>(tv, q, node)) <= rr) {
       cnt += m.count;  // whole subtree inside the ball
       cov_lo = m.start;
       cov_hi = m.start + m.count;

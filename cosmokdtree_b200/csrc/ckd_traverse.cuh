@@ -1,5 +1,7 @@
 // ckd_traverse.cuh -- per-lane distance helpers and the query ordering pass.
 #pragma once
+#include <math_constants.h>
+
 #include "ckd_common.cuh"
 
 namespace ckd {
@@ -43,6 +45,28 @@ __device__ __forceinline__ double box_maxd2(const TreeView& tv, const double (&q
     double a = fabs(dsub(q[j], __ldg(&b[2 * j])));
     double c = fabs(dsub(q[j], __ldg(&b[2 * j + 1])));
     double g = a > c ? a : c;
+    s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
+  }
+  return s;
+}
+
+// Periodic form of box_maxd2 for the "whole subtree inside the ball" shortcut:
+// the direct (unwrapped) upper bound, valid when on every axis both faces lie
+// within L/2 of q -- then every point's minimum-image difference is its direct
+// difference (min(a, L - a) = a for a <= L/2, also after rounding), so each
+// point's computed squared distance is at most this bound.  Returns +inf when
+// some axis fails the condition.
+template <int D>
+__device__ __forceinline__ double box_maxd2_near(const TreeView& tv, const double (&q)[D],
+                                                 int32_t node) {
+  const double* b = tv.box + (int64_t)node * 2 * D;
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double a = fabs(dsub(q[j], __ldg(&b[2 * j])));
+    double c = fabs(dsub(q[j], __ldg(&b[2 * j + 1])));
+    double g = a > c ? a : c;
+    if (!(g <= 0.5 * tv.L[j])) return CUDART_INF;
     s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
   }
   return s;

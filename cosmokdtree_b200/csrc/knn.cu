@@ -840,6 +840,9 @@ __global__ void __launch_bounds__(128) k_knn_lane(TreeView tv, const double* __r
 // recomputed once for the output.  8 bytes per entry instead of 12 lets 1.5x
 // more warps stay resident; heap comparisons are 32-bit.  Sentinels: position -1
 // = (HUGE, id -1), position -2 = (r2, INT32_MAX) for the bounded search.
+// shared memory of the compact per-lane kernel per warp: k heap slots (1-based) x 32 lanes
+__host__ __device__ inline size_t compact_heap_bytes(int k) { return (size_t)(k + 1) * 32 * 8; }
+
 constexpr int32_t kPosMissing = -1;
 constexpr int32_t kPosBound = -2;
 
@@ -862,10 +865,6 @@ struct CompactCtx {
   }
 };
 
-__device__ __forceinline__ float f32_above(float x) {  // next float up (x finite, >= 0)
-  return __uint_as_float(__float_as_uint(x) + 1u);
-}
-
 template <int D, bool PER, bool BOUNDED = false>
 __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double* __restrict__ Q,
                                                    const int32_t* __restrict__ order, int64_t nq,
@@ -882,9 +881,11 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int KS = heap_stride(k);
-  float* keys = reinterpret_cast<float*>(smem) + (size_t)w * 32 * KS;
-  int32_t* poss = reinterpret_cast<int32_t*>(smem) + (size_t)nw * 32 * KS + (size_t)w * 32 * KS;
+  // heap slot s of this lane at H[s * 32 + lane]: (key bits, position); keys are
+  // non-negative floats, so their bit patterns order as unsigned integers, and
+  // every lane always addresses its own bank pair (no conflicts between lanes
+  // at different heap levels)
+  uint2* H = reinterpret_cast<uint2*>(smem) + (size_t)w * 32 * (k + 1) + lane;
   const int64_t gw = (int64_t)blockIdx.x * nw + w;
   const int64_t slot = gw * 32 + lane;
   const bool valid = slot < nq;
@@ -897,8 +898,6 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
     qs.q32[j] = __double2float_rn(q[j]);
     qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
   }
-  float* hk = keys + lane * KS;
-  int32_t* hp = poss + lane * KS;
   float skey = FLT_MAX;
   int32_t spos = kPosMissing;
   float wd32 = FLT_MAX;
@@ -913,12 +912,9 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
     }
   }
   const CompactCtx<D, PER> cx{tv, q, rr};
-  for (int s = 1; s <= k; ++s) {
-    hk[s] = skey;
-    hp[s] = spos;
-  }
-  float wk = skey;      // root key
-  int32_t wp = spos;    // root position
+  for (int s = 1; s <= k; ++s) H[s * 32] = make_uint2(__float_as_uint(skey), (unsigned)spos);
+  unsigned wk = __float_as_uint(skey);  // root key bits
+  int32_t wp = spos;                    // root position
 
   int32_t sn[kLaneStack];
   float sd[kLaneStack];
@@ -1024,7 +1020,7 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
         mask &= mask - 1;
         const int32_t p = p0 + i;
         const double d2 = point_d2<D, PER>(tv, q, p);
-        const float kc = __double2float_rn(d2);
+        const unsigned kc = __float_as_uint(__double2float_rn(d2));
         if (kc > wk) continue;
         if (kc == wk) {  // FP32 tie with the root: exact comparison
           const double dr = cx.exact(wp);
@@ -1037,21 +1033,17 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
         for (;;) {
           const int l = 2 * s;
           if (l > k) break;
-          float kch;
-          int32_t pch;
-          int c;
+          uint2 ch = H[l * 32];
+          int c = l;
           if (l < k) {
-            const float2 kk = *reinterpret_cast<const float2*>(hk + l);
-            const int2 pp = *reinterpret_cast<const int2*>(hp + l);
-            const bool right = kk.x < kk.y || (kk.x == kk.y && cx.tie_before(pp.x, pp.y));
-            kch = right ? kk.y : kk.x;
-            pch = right ? pp.y : pp.x;
-            c = right ? l + 1 : l;
-          } else {
-            kch = hk[l];
-            pch = hp[l];
-            c = l;
+            const uint2 r = H[(l + 1) * 32];
+            if (ch.x < r.x || (ch.x == r.x && cx.tie_before((int32_t)ch.y, (int32_t)r.y))) {
+              ch = r;
+              c = l + 1;
+            }
           }
+          const unsigned kch = ch.x;
+          const int32_t pch = (int32_t)ch.y;
           // the candidate stays above the child iff it ranks after it
           bool cand_before = kc < kch;
           if (kc == kch) {
@@ -1059,15 +1051,14 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
             cand_before = d2 < dch || (d2 == dch && __ldg(&tv.ids[p]) < cx.id(pch));
           }
           if (!cand_before) break;
-          hk[s] = kch;
-          hp[s] = pch;
+          H[s * 32] = ch;
           s = c;
         }
-        hk[s] = kc;
-        hp[s] = p;
-        wk = hk[1];
-        wp = hp[1];
-        wd32 = f32_above(wk);
+        H[s * 32] = make_uint2(kc, (unsigned)p);
+        const uint2 root = H[32];
+        wk = root.x;
+        wp = (int32_t)root.y;
+        wd32 = __uint_as_float(wk + 1u);
       }
     }
     // ---- next: pop the nearest pending subtree still within reach
@@ -1101,33 +1092,26 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
   }
   if (sorted && valid && !missed) {
     for (int end = k; end > 1; --end) {
-      const float key = hk[end];
-      const int32_t pk = hp[end];
-      hk[end] = hk[1];
-      hp[end] = hp[1];
+      const uint2 e = H[end * 32];
+      H[end * 32] = H[32];
       int s = 1;
       for (;;) {
         const int l = 2 * s;
         if (l >= end) break;
         int c = l;
-        float kc = hk[l];
-        int32_t pc = hp[l];
+        uint2 ch = H[l * 32];
         if (l + 1 < end) {
-          const float kr = hk[l + 1];
-          const int32_t pr = hp[l + 1];
-          if (kc < kr || (kc == kr && cx.tie_before(pc, pr))) {
+          const uint2 r = H[(l + 1) * 32];
+          if (ch.x < r.x || (ch.x == r.x && cx.tie_before((int32_t)ch.y, (int32_t)r.y))) {
             c = l + 1;
-            kc = kr;
-            pc = pr;
+            ch = r;
           }
         }
-        if (!(key < kc || (key == kc && cx.tie_before(pk, pc)))) break;
-        hk[s] = kc;
-        hp[s] = pc;
+        if (!(e.x < ch.x || (e.x == ch.x && cx.tie_before((int32_t)e.y, (int32_t)ch.y)))) break;
+        H[s * 32] = ch;
         s = c;
       }
-      hk[s] = key;
-      hp[s] = pk;
+      H[s * 32] = e;
     }
   }
   __syncwarp();
@@ -1140,9 +1124,9 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
     for (int j = 0; j < D; ++j) qx[j] = __shfl_sync(FULL, q[j], qq);
     if (BOUNDED && ((missmask >> qq) & 1u)) continue;
     const int64_t row = order ? (int64_t)order[s2] : s2;
-    const int32_t* rp = poss + qq * KS + 1;
+    const uint2* rp = H - lane + qq + 32;  // query qq's slot 1
     for (int j = lane; j < k; j += 32) {
-      const int32_t p = rp[j];
+      const int32_t p = (int32_t)rp[j * 32].y;
       double d2 = CKD_HUGE;
       int64_t id = -2;
       if (p >= 0) {
@@ -2519,7 +2503,7 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
   if (k <= kSmemK && t->screen_ok && (var == 0 || var == 7) && t->depth < kLaneStack - 1) {
     const int nw7 = std::min(4, knn_warps_per_block());
     const unsigned blocks7 = (unsigned)cdiv(cdiv(nq, 32), nw7);
-    size_t sm = (size_t)nw7 * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    size_t sm = (size_t)nw7 * compact_heap_bytes(k);
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
     CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2755,7 +2739,7 @@ ckd_status forest_knn_impl(const ckd_tree* t, const double* q, const int32_t* qr
   if (st == CKD_OK) {
     const int nw = std::min(4, knn_warps_per_block());
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
-    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    size_t sm = (size_t)nw * compact_heap_bytes(k);
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
     cudaError_t e = cudaFuncSetAttribute(k_knn_lane2<D, PER>,
@@ -2826,7 +2810,7 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
   if (st == CKD_OK && learned_kernel() == 0) {
     const int nw = std::min(4, knn_warps_per_block());
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
-    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    size_t sm = (size_t)nw * compact_heap_bytes(k);
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
     cudaError_t e = cudaFuncSetAttribute(k_knn_lane2<D, PER, true>,
@@ -3011,7 +2995,7 @@ ckd_status knn_noalloc_impl(const ckd_tree* t, const double* q, int64_t nq, int 
   const int nw = 4;
   const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
   if (t->screen_ok && t->depth < kLaneStack - 1) {
-    size_t sm = (size_t)nw * heap_stride(k) * 32 * (sizeof(float) + sizeof(int32_t));
+    size_t sm = (size_t)nw * compact_heap_bytes(k);
     CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm));
     k_knn_lane2<D, PER><<<blocks, nw * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
