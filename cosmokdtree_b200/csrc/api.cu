@@ -35,7 +35,7 @@ int knn_variant() { return g_knn_variant.load(std::memory_order_relaxed); }
 static std::atomic<int> g_knn_bps{0}, g_knn_wpb{2};
 int knn_blocks_per_sm() { return g_knn_bps.load(std::memory_order_relaxed); }
 int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
-static std::atomic<int> g_learned_kernel{0}, g_gather_wpb{2};
+static std::atomic<int> g_learned_kernel{3}, g_gather_wpb{2};
 int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); }
 int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
 static std::atomic<int> g_order_mode{0};
@@ -413,7 +413,7 @@ int64_t ckd_launch_count(void) { return g_launches.load(); }
 ckd_status ckd_knn_stats(int enable, int64_t* out8) { return knn_stats(enable, out8); }
 
 ckd_status ckd_set_knn_variant(int variant) {
-  if (variant < 0 || variant > 7) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..7");
+  if (variant < 0 || variant > 8) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..8");
   g_knn_variant.store(variant);
   return CKD_OK;
 }
@@ -448,7 +448,7 @@ ckd_status ckd_set_tuning(int key, int value) {
       set_knn_bucket_alpha(value / 100.0f);
       return CKD_OK;
     case 4:
-      if (value < 0 || value > 2) return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0, 1 or 2");
+      if (value < 0 || value > 3) return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0..3");
       g_learned_kernel.store(value);
       return CKD_OK;
     case 5:

@@ -43,7 +43,8 @@ int knn_variant();
 int knn_blocks_per_sm();
 int knn_warps_per_block();
 // learned-bound search kernel: 0 bounded per-lane with compact heap (k_knn_lane2),
-// 1 warp gather, 2 bounded per-lane with the wide heap (k_knn_lane);
+// 1 warp gather, 2 bounded per-lane with the wide heap (k_knn_lane), 3 as 0 with
+// child-pair-record descent (default);
 // warps per block of the gather kernel
 int learned_kernel();
 int gather_warps_per_block();

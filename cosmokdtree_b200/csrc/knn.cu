@@ -311,6 +311,29 @@ __device__ __forceinline__ float node_mind_lb(const TreeView& tv, const QueryScr
   return s * kShrink;
 }
 
+// node_mind_lb for a box held in registers (lo/hi padded to a multiple of 4)
+template <int D, bool PER, int W>
+__device__ __forceinline__ float box_mind_lb(const TreeView& tv, const QueryScreen<D, PER>& qs,
+                                             const float (&lo)[W], const float (&hi)[W]) {
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float x = qs.q32[j], g;
+    if (x >= lo[j] - qs.dlt[j] && x <= hi[j] + qs.dlt[j]) {
+      g = 0.0f;
+    } else if (!PER) {
+      g = fmaxf(lo[j] - x, x - hi[j]) - qs.dlt[j];
+    } else {
+      float L = (float)tv.L[j];
+      float t1 = fabsf(x - lo[j]), t2 = fabsf(x - hi[j]);
+      g = fminf(fminf(t1, L - t1), fminf(t2, L - t2)) - qs.dlt[j];
+    }
+    g = fmaxf(g, 0.0f);
+    s = fmaf(g, g, s);
+  }
+  return s * kShrink;
+}
+
 template <int D, bool PER>
 __global__ void __launch_bounds__(128) k_knn_screen(TreeView tv, const double* __restrict__ Q,
                                                     const int32_t* __restrict__ order, int64_t nq,
@@ -865,7 +888,7 @@ struct CompactCtx {
   }
 };
 
-template <int D, bool PER, bool BOUNDED = false>
+template <int D, bool PER, bool BOUNDED = false, bool PAIR = false>
 __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double* __restrict__ Q,
                                                    const int32_t* __restrict__ order, int64_t nq,
                                                    int k, int sorted, double* __restrict__ dist,
@@ -938,35 +961,89 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
     }
     node = a < 0 ? node : a;
   }
+  // PAIR: stack entries and `node` carry the leaf flag (a leaf is stored as ~id,
+  // < -1 because children ids are >= 1; -1 means "no node") and internal nodes are
+  // expanded from their child-pair record alone (both children's FP32 boxes, ids
+  // and leaf flags), one dependent load per level.  Otherwise the node's meta is
+  // read first, then both children's FP32 boxes.
+  constexpr int PF = pair_f4(D);
+  bool is_leaf = node >= 0 && PAIR && load_meta(tv.meta, node).left < 0;
+  NodeMeta m;
   while (node >= 0) {
     // ---- descend to a leaf, nearer child first
-    NodeMeta m = load_meta(tv.meta, node);
-    while (node >= 0 && m.left >= 0) {
-      if (stats) st[0] += 1;
-      float ml = node_mind_lb<D, PER>(tv, qs, m.left);
-      float mr = node_mind_lb<D, PER>(tv, qs, m.left + 1);
-      bool nl = ml <= wd32, nr = mr <= wd32;
-      if (nl && nr) {
-        bool lf = ml <= mr;
-        sn[top] = lf ? m.left + 1 : m.left;
-        sd[top] = lf ? mr : ml;
-        ++top;
-        node = lf ? m.left : m.left + 1;
-      } else if (nl || nr) {
-        node = nl ? m.left : m.left + 1;
-      } else {
-        node = -1;
-        while (top > 0) {
-          --top;
-          if (sd[top] <= wd32) {
-            node = sn[top];
-            break;
+    if (!PAIR) {
+      m = load_meta(tv.meta, node);
+      while (node >= 0 && m.left >= 0) {
+        if (stats) st[0] += 1;
+        const float ml = node_mind_lb<D, PER>(tv, qs, m.left);
+        const float mr = node_mind_lb<D, PER>(tv, qs, m.left + 1);
+        const bool nl = ml <= wd32, nr = mr <= wd32;
+        if (nl && nr) {
+          const bool lf = ml <= mr;
+          sn[top] = lf ? m.left + 1 : m.left;
+          sd[top] = lf ? mr : ml;
+          ++top;
+          node = lf ? m.left : m.left + 1;
+        } else if (nl || nr) {
+          node = nl ? m.left : m.left + 1;
+        } else {
+          node = -1;
+          while (top > 0) {
+            --top;
+            if (sd[top] <= wd32) {
+              node = sn[top];
+              break;
+            }
           }
         }
+        if (node >= 0) m = load_meta(tv.meta, node);
       }
-      if (node >= 0) m = load_meta(tv.meta, node);
+      if (node < 0) break;
+    } else {
+      while (!is_leaf) {
+        if (stats) st[0] += 1;
+        const float4* rec = tv.pair + (int64_t)node * PF;
+        float lo_l[4 * NV], hi_l[4 * NV], lo_r[4 * NV], hi_r[4 * NV];
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+          const float4 a = __ldg(rec + h), b = __ldg(rec + NV + h);
+          const float4 c = __ldg(rec + 2 * NV + h), d = __ldg(rec + 3 * NV + h);
+          lo_l[4 * h] = a.x; lo_l[4 * h + 1] = a.y; lo_l[4 * h + 2] = a.z; lo_l[4 * h + 3] = a.w;
+          hi_l[4 * h] = b.x; hi_l[4 * h + 1] = b.y; hi_l[4 * h + 2] = b.z; hi_l[4 * h + 3] = b.w;
+          lo_r[4 * h] = c.x; lo_r[4 * h + 1] = c.y; lo_r[4 * h + 2] = c.z; lo_r[4 * h + 3] = c.w;
+          hi_r[4 * h] = d.x; hi_r[4 * h + 1] = d.y; hi_r[4 * h + 2] = d.z; hi_r[4 * h + 3] = d.w;
+        }
+        const int4 info = __ldg(reinterpret_cast<const int4*>(rec + 4 * NV));
+        const float ml = box_mind_lb<D, PER>(tv, qs, lo_l, hi_l);
+        const float mr = box_mind_lb<D, PER>(tv, qs, lo_r, hi_r);
+        const bool nl = ml <= wd32, nr = mr <= wd32;
+        const int32_t el = info.z ? ~info.x : info.x, er = info.w ? ~info.y : info.y;
+        int32_t nxt = -1;
+        if (nl && nr) {
+          const bool lf = ml <= mr;
+          sn[top] = lf ? er : el;
+          sd[top] = lf ? mr : ml;
+          ++top;
+          nxt = lf ? el : er;
+        } else if (nl || nr) {
+          nxt = nl ? el : er;
+        } else {
+          while (top > 0) {
+            --top;
+            if (sd[top] <= wd32) {
+              nxt = sn[top];
+              break;
+            }
+          }
+          if (nxt == -1) break;
+        }
+        is_leaf = nxt < 0;
+        node = is_leaf ? ~nxt : nxt;
+      }
+      if (!is_leaf) break;
+      m = load_meta(tv.meta, node);
     }
-    if (node < 0) break;
+
     // ---- scan the leaf
     if (stats) {
       st[2] += 1;
@@ -1062,13 +1139,20 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
       }
     }
     // ---- next: pop the nearest pending subtree still within reach
-    node = -1;
+    int32_t nxt = -1;
     while (top > 0) {
       --top;
       if (sd[top] <= wd32) {
-        node = sn[top];
+        nxt = sn[top];
         break;
       }
+    }
+    if (nxt == -1) break;
+    if (PAIR) {
+      is_leaf = nxt < 0;
+      node = is_leaf ? ~nxt : nxt;
+    } else {
+      node = nxt;
     }
   }
   if (stats) {
@@ -2500,16 +2584,24 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
   bool use_gstack = stack_len > kStack || k > kSmemK;
   if (use_gstack)
     CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
-  if (k <= kSmemK && t->screen_ok && (var == 0 || var == 7) && t->depth < kLaneStack - 1) {
+  if (k <= kSmemK && t->screen_ok && (var == 0 || var == 7 || var == 8) &&
+      t->depth < kLaneStack - 1) {
     const int nw7 = std::min(4, knn_warps_per_block());
     const unsigned blocks7 = (unsigned)cdiv(cdiv(nq, 32), nw7);
     size_t sm = (size_t)nw7 * compact_heap_bytes(k);
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
-    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sm));
-    k_knn_lane2<D, PER><<<blocks7, nw7 * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
-                                                      knn_stats_buffer());
+    if (var == 8) {
+      CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER, false, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_knn_lane2<D, PER, false, true><<<blocks7, nw7 * 32, sm, s>>>(
+          tv, q, order, nq, k, sorted, dist, idx, knn_stats_buffer());
+    } else {
+      CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_knn_lane2<D, PER><<<blocks7, nw7 * 32, sm, s>>>(tv, q, order, nq, k, sorted, dist, idx,
+                                                        knn_stats_buffer());
+    }
     CKD_LAUNCH_CHECK();
     if (gstack) CKD_CUDA(dev_free(gstack, s));
     return CKD_OK;
@@ -2807,18 +2899,25 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     timing_begin(s);
     st = mlp_radius(t, net, q, order, qleaf, nq, k, r2, s);
   }
-  if (st == CKD_OK && learned_kernel() == 0) {
+  if (st == CKD_OK && (learned_kernel() == 0 || learned_kernel() == 3)) {
     const int nw = std::min(4, knn_warps_per_block());
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
     size_t sm = (size_t)nw * compact_heap_bytes(k);
     const int bps = knn_blocks_per_sm();
     if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
-    cudaError_t e = cudaFuncSetAttribute(k_knn_lane2<D, PER, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const bool pair = learned_kernel() == 3;
+    cudaError_t e = pair ? cudaFuncSetAttribute(k_knn_lane2<D, PER, true, true>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)
+                         : cudaFuncSetAttribute(k_knn_lane2<D, PER, true>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_knn_lane2)");
-    k_knn_lane2<D, PER, true><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted,
-                                                          dist, idx, knn_stats_buffer(), r2, miss,
-                                                          nmiss, qleaf);
+    if (pair)
+      k_knn_lane2<D, PER, true, true><<<blocks, nw * 32, sm, s>>>(
+          t->view(), q, order, nq, k, sorted, dist, idx, knn_stats_buffer(), r2, miss, nmiss, qleaf);
+    else
+      k_knn_lane2<D, PER, true><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted,
+                                                            dist, idx, knn_stats_buffer(), r2,
+                                                            miss, nmiss, qleaf);
     note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) st = cuda_fail(e, "k_knn_lane2 (bounded)");

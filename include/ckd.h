@@ -102,7 +102,8 @@ int64_t ckd_launch_count(void);
  * traversal, 3 = per-lane traversal with 12-byte heap entries, 4 = bottom-up
  * per-lane search, 5 = persistent per-lane search, 6 = warp per bucket with a
  * density radius, 7 = per-lane traversal with 8-byte heap entries (FP32 key +
- * position, exact tie resolution).  Every variant returns the same exact result. */
+ * position, exact tie resolution), 8 = 7 expanding nodes from child-pair records.
+ * Every variant returns the same exact result. */
 ckd_status ckd_set_knn_variant(int variant);
 
 /* Process-wide launch tuning of the search kernels (no reference counterpart;
@@ -112,8 +113,8 @@ ckd_status ckd_set_knn_variant(int variant);
  * of the kNN kernel (1..8, default 2; the per-lane kernels use at most 4); key 3: radius factor of the warp-per-bucket
  * kNN search in hundredths (default 150 = 1.5x the density estimate); key 4:
  * search kernel of ckd_knn_learned (0 = bounded per-lane traversal with 8-byte
- * heap entries, default; 1 = warp gather; 2 = bounded per-lane with 12-byte
- * entries); key 5: warps per block of the warp-gather kernel (1..4, default 2);
+ * heap entries; 1 = warp gather; 2 = bounded per-lane with 12-byte entries; 3 = 0
+ * with child-pair-record descent, default); key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
  * default; 1 = always; 2 = never). */
 ckd_status ckd_set_tuning(int key, int value);

@@ -83,12 +83,13 @@ def test_features_match_numpy(gpu):
     np.testing.assert_allclose(f, ref, rtol=0, atol=2e-4)
 
 
-@pytest.fixture(params=[0, 1, 2], ids=["bounded_lane_compact", "gather", "bounded_lane_wide"])
+@pytest.fixture(params=[0, 1, 2, 3],
+                ids=["bounded_lane_compact", "gather", "bounded_lane_wide", "bounded_lane_pair"])
 def learned_kernel(request, gpu):
     from cosmokdtree_b200 import _lib
     _lib.check(_lib.load().ckd_set_tuning(4, request.param))
     yield request.param
-    _lib.load().ckd_set_tuning(4, 0)
+    _lib.load().ckd_set_tuning(4, 3)
 
 
 @pytest.mark.parametrize("k", [8, 32])

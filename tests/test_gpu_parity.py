@@ -112,9 +112,9 @@ KNN_CASES = [
 ]
 
 
-@pytest.fixture(params=[1, 2, 3, 4, 5, 6, 7],
+@pytest.fixture(params=[1, 2, 3, 4, 5, 6, 7, 8],
                 ids=["fp64", "screened", "lane", "bottom_up", "persistent", "bucket",
-                     "lane_compact"])
+                     "lane_compact", "lane_compact_pair"])
 def knn_variant(request, gpu):
     from cosmokdtree_b200 import _lib
     _lib.check(_lib.load().ckd_set_knn_variant(request.param))
