@@ -60,6 +60,9 @@ struct BuildBufs {
   int32_t* tile_sum = nullptr;
   int32_t* tile_off = nullptr;
   int32_t* scal = nullptr;  // device scalars: [0] next open count, [1] error flag
+  // per tile of kTile positions: 1 if the tile holds a position of an open node
+  // this level (the tile kernels return at once for the other tiles)
+  unsigned char* tile_act = nullptr;
 };
 
 // ------------------------------------------------------------------ kernels
@@ -97,6 +100,17 @@ __device__ __forceinline__ bool open_node(const NodeMeta* __restrict__ meta, int
   return m.depth == level && m.count > leaf;
 }
 
+// tile_act[t] = 1 for every tile that a segment of an open node overlaps
+__global__ void k_mark_tiles(const int32_t* __restrict__ act, int m,
+                             const NodeMeta* __restrict__ meta,
+                             unsigned char* __restrict__ tile_act) {
+  const int i = blockIdx.x;
+  if (i >= m) return;
+  const NodeMeta nm = meta[act[i]];
+  const int64_t t0 = nm.start / kTile, t1 = ((int64_t)nm.start + nm.count - 1) / kTile;
+  for (int64_t t = t0 + threadIdx.x; t <= t1; t += blockDim.x) tile_act[t] = 1;
+}
+
 // Segmented min/max over open positions; one atomicMin/atomicMax per segment
 // piece that crosses a warp-chunk boundary, direct atomics for pieces inside.
 template <int D>
@@ -104,7 +118,9 @@ __global__ void __launch_bounds__(kBT) k_seg_box(const double* __restrict__ X,
                                                  const int32_t* __restrict__ NID,
                                                  const NodeMeta* __restrict__ meta, int level,
                                                  int leaf, int64_t n,
-                                                 unsigned long long* __restrict__ keys) {
+                                                 unsigned long long* __restrict__ keys,
+                                                 const unsigned char* __restrict__ tile_act) {
+  if (tile_act && !tile_act[blockIdx.x]) return;
   constexpr int W = kBT / 32;
   __shared__ int32_t rec_id[kItems * W][2];
   __shared__ unsigned long long rec_v[kItems * W][2][2 * D];
@@ -266,9 +282,11 @@ __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __res
 // first position of a sliding segment that holds the extreme value
 __global__ void k_argext(const double* __restrict__ X, const int32_t* __restrict__ NID,
                          const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
-                         int level, int leaf, int64_t n, int32_t* __restrict__ ext) {
+                         int level, int leaf, int64_t n, int32_t* __restrict__ ext,
+                         const unsigned char* __restrict__ tile_act) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
+  if (!tile_act[p / kTile]) return;
   int32_t a = NID[p];
   if (!open_node(meta, a, level, leaf)) return;
   if (mode[a] == 0) return;
@@ -291,8 +309,13 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ ext, int level, int leaf,
                                                int64_t n, int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
-                                               int32_t* __restrict__ pend) {
+                                               int32_t* __restrict__ pend,
+                                               const unsigned char* __restrict__ tile_act) {
   __shared__ int32_t tmp[kBT / 32];
+  if (!tile_act[blockIdx.x]) {
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = 0;
+    return;
+  }
   const int64_t base = (int64_t)blockIdx.x * kTile;
   int32_t run = 0;
   for (int it = 0; it < kItems; ++it) {
@@ -389,8 +412,10 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     const int32_t* __restrict__ ext, const int32_t* __restrict__ tile_off,
     const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase, int level, int leaf,
     int64_t n, double* __restrict__ Xo, int32_t* __restrict__ Io, int32_t* __restrict__ NIDo,
-    double* __restrict__ Pf, int32_t* __restrict__ If, int32_t* __restrict__ err) {
+    double* __restrict__ Pf, int32_t* __restrict__ If, int32_t* __restrict__ err,
+    const unsigned char* __restrict__ tile_act) {
   __shared__ int32_t tmp[kBT / 32];
+  if (!tile_act[blockIdx.x]) return;
   const int64_t base = (int64_t)blockIdx.x * kTile;
   int32_t run = tile_off[blockIdx.x];
   for (int it = 0; it < kItems; ++it) {
@@ -605,7 +630,7 @@ void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
                 B.nleft,  B.pbase,   B.act[0],    B.act[1],   B.nxt_cnt, B.nxt_off, B.tile_sum,
-                B.tile_off, B.scal};
+                B.tile_off, B.scal, B.tile_act};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -637,6 +662,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(dev_alloc((void**)&B.tile_sum, sizeof(int32_t) * ntiles, s));
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
+  CKD_CUDA(dev_alloc((void**)&B.tile_act, (size_t)ntiles, s));
   CKD_CUDA(cudaMemsetAsync(B.scal, 0, sizeof(int32_t) * 4, s));
 
   // final outputs
@@ -671,7 +697,8 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   // Root bounding boxes: validation (finite, inside the periodic box) and the
   // non-periodic root cells.  Computed with the open-node reduction using a leaf
   // threshold of 0 so that every root is "open" here.
-  k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], B.meta, 0, 0, n, B.keys);
+  k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], B.meta, 0, 0, n, B.keys,
+                                                 nullptr);
   CKD_LAUNCH_CHECK();
   std::vector<unsigned long long> rk((size_t)T * 2 * D);
   CKD_CUDA(cudaMemcpyAsync(rk.data(), B.keys, sizeof(unsigned long long) * 2 * D * T,
@@ -734,18 +761,21 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     CKD_TRY(ensure_node_cap(B, (int64_t)n_nodes + 2 * (int64_t)m, s));
     const int32_t* act = B.act[cur];
     unsigned gm = (unsigned)cdiv(m, 128);
+    CKD_CUDA(cudaMemsetAsync(B.tile_act, 0, (size_t)ntiles, s));
+    k_mark_tiles<<<(unsigned)m, 128, 0, s>>>(act, m, B.meta, B.tile_act);
+    CKD_LAUNCH_CHECK();
     if (level > 0) {
       k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, level, leaf, n,
-                                                    B.keys);
+                                                    B.keys, B.tile_act);
       CKD_LAUNCH_CHECK();
     }
     k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
     CKD_LAUNCH_CHECK();
     k_argext<<<(unsigned)cdiv(n, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, level,
-                                                    leaf, n, B.ext);
+                                                    leaf, n, B.ext, B.tile_act);
     CKD_LAUNCH_CHECK();
     k_flags<<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, level,
-                                             leaf, n, B.tile_sum, B.pstart, B.pend);
+                                             leaf, n, B.tile_sum, B.pstart, B.pend, B.tile_act);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntiles, s));
     k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off,
@@ -757,7 +787,8 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     CKD_LAUNCH_CHECK();
     k_scatter<D><<<(unsigned)ntiles, kBT, 0, s>>>(
         B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext, B.tile_off, B.nleft, B.pbase,
-        level, leaf, n, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
+        level, leaf, n, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1,
+        B.tile_act);
     CKD_LAUNCH_CHECK();
     int32_t nm = 0;
     CKD_CUDA(cudaMemcpyAsync(&nm, B.nxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
