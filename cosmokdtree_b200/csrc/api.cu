@@ -40,6 +40,8 @@ int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); 
 int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
 static std::atomic<int> g_order_mode{0};
 int query_order_mode() { return g_order_mode.load(std::memory_order_relaxed); }
+static std::atomic<int> g_mlp_tc{0};
+bool mlp_tensor_cores() { return g_mlp_tc.load(std::memory_order_relaxed) != 0; }
 void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -458,6 +460,10 @@ ckd_status ckd_set_tuning(int key, int value) {
     case 6:
       if (value < 0 || value > 2) return fail(CKD_ERR_BAD_ARG, "query ordering must be 0, 1 or 2");
       g_order_mode.store(value);
+      return CKD_OK;
+    case 7:
+      if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "MLP inference path must be 0 or 1");
+      g_mlp_tc.store(value);
       return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");

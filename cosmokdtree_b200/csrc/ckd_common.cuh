@@ -50,6 +50,8 @@ int learned_kernel();
 int gather_warps_per_block();
 // query leaf ordering before a search: 0 automatic, 1 always, 2 never
 int query_order_mode();
+// learned-bound network inference on the tensor cores (tcgen05) instead of FP32 FMAs
+bool mlp_tensor_cores();
 
 // events bracketing the main search kernel when kernel timing is on
 void timing_begin(cudaStream_t s);

@@ -116,7 +116,8 @@ ckd_status ckd_set_knn_variant(int variant);
  * heap entries; 1 = warp gather; 2 = bounded per-lane with 12-byte entries; 3 = 0
  * with child-pair-record descent, default); key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
- * default; 1 = always; 2 = never). */
+ * default; 1 = always; 2 = never); key 7: inference of the learned-bound network
+ * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference

@@ -62,6 +62,20 @@ def forward(w, norm, X, rounded=True):
     return z, (xh, a1, h1, a2, h2)
 
 
+def predict_bf16_activations(w, norm, X):
+    """Prediction with BF16 inputs to both hidden layers' products (the tensor-core
+    inference path): standardised features and first-layer activations rounded to
+    BF16, products accumulated exactly, biases / ReLU / output layer in FP64."""
+    norm = np.asarray(norm, dtype=np.float32)
+    w1, b1, w2, b2, w3, b3 = unpack(bf16_round(w))
+    xh = bf16_round(((np.asarray(X, np.float32) - norm[:F]) * norm[F:2 * F]).astype(np.float32))
+    h1 = np.maximum(xh.astype(np.float64) @ w1.T + b1, 0.0)
+    h1b = bf16_round(h1.astype(np.float32)).astype(np.float64)
+    h2 = np.maximum(h1b @ w2.T + b2, 0.0)
+    z = h2 @ w3 + b3
+    return float(norm[2 * F]) + float(norm[2 * F + 1]) * z
+
+
 def predict(w, norm, X):
     """log2 k-th distance prediction y = t_mu + t_sigma * z (FP64)."""
     norm = np.asarray(norm, dtype=np.float32)

@@ -171,3 +171,35 @@ def test_learned_bound_saves_work(trained):
     assert learned[6] < 0.8 * plain[6], (learned, plain)
     assert learned[0] < 0.9 * plain[0], (learned, plain)
     assert learned[5] < plain[5], (learned, plain)
+
+
+def test_tensor_core_inference_matches_reference(gpu):
+    """The tcgen05 inference kernel against the FP64 reference with BF16
+    activations, and the learned search through it stays exact."""
+    from cosmokdtree_b200 import _lib, kdtree
+    from cosmokdtree_b200.learned import LearnedBound
+    L = _lib.load()
+    P = _catalogue(60_000, 49)
+    t = kdtree.build_kdtree(P, leaf=16, boxsize=1.0)
+    rng = np.random.default_rng(50)
+    lb = LearnedBound(seed=11)
+    lb.fit(t, P[rng.integers(0, len(P), 20_000)], [8, 32], epochs=4, batch=1024)
+    Q = np.concatenate([P[rng.integers(0, len(P), 3000)], rng.random((333, 3)) - 0.5])
+    feat = lb.features(t, Q, 16)
+    sd = lb.state_dict()
+    X = feat.cpu().numpy()
+    y_simt = lb.predict(feat).cpu().numpy()
+    _lib.check(L.ckd_set_tuning(7, 1))
+    try:
+        y_tc = lb.predict(feat).cpu().numpy()
+        ref = M.predict_bf16_activations(sd["params"], sd["norm"], X)
+        np.testing.assert_allclose(y_tc, ref, rtol=0, atol=2e-2)
+        assert np.median(np.abs(y_tc - ref)) < 1e-3
+        assert np.abs(y_tc - y_simt).max() < 0.1  # BF16 activations move predictions slightly
+        for k in (8, 32):
+            d1, i1 = lb.knn(t, Q, k)
+            d0, i0 = kdtree.knn_search(t, Q, k)
+            np.testing.assert_array_equal(i1, i0)
+            np.testing.assert_array_equal(d1, d0)
+    finally:
+        _lib.check(L.ckd_set_tuning(7, 0))
