@@ -40,7 +40,7 @@ int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); 
 int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
 static std::atomic<int> g_order_mode{0};
 int query_order_mode() { return g_order_mode.load(std::memory_order_relaxed); }
-static std::atomic<int> g_mlp_tc{0};
+static std::atomic<int> g_mlp_tc{1};
 bool mlp_tensor_cores() { return g_mlp_tc.load(std::memory_order_relaxed) != 0; }
 void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }

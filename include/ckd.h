@@ -117,7 +117,7 @@ ckd_status ckd_set_knn_variant(int variant);
  * with child-pair-record descent, default); key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
  * default; 1 = always; 2 = never); key 7: inference of the learned-bound network
- * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations). */
+ * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations, default). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference

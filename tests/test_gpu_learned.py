@@ -57,8 +57,13 @@ def test_gradient_matches_cpu_reference(gpu):
     assert loss2 < loss
     assert np.isclose(loss2, lref2, rtol=1e-4)
     np.testing.assert_allclose(g2, gref2, rtol=2e-3, atol=1e-4 * np.abs(gref2).max())
-    # inference kernel against the FP64 forward pass
-    y = lb.predict(feat).cpu().numpy()
+    # FP32 inference kernel against the FP64 forward pass
+    from cosmokdtree_b200 import _lib
+    _lib.check(_lib.load().ckd_set_tuning(7, 0))
+    try:
+        y = lb.predict(feat).cpu().numpy()
+    finally:
+        _lib.check(_lib.load().ckd_set_tuning(7, 1))
     np.testing.assert_allclose(y, M.predict(sd2["params"], sd2["norm"], X), rtol=0, atol=2e-4)
     del torch
 
@@ -188,6 +193,7 @@ def test_tensor_core_inference_matches_reference(gpu):
     feat = lb.features(t, Q, 16)
     sd = lb.state_dict()
     X = feat.cpu().numpy()
+    _lib.check(L.ckd_set_tuning(7, 0))
     y_simt = lb.predict(feat).cpu().numpy()
     _lib.check(L.ckd_set_tuning(7, 1))
     try:
@@ -202,4 +208,4 @@ def test_tensor_core_inference_matches_reference(gpu):
             np.testing.assert_array_equal(i1, i0)
             np.testing.assert_array_equal(d1, d0)
     finally:
-        _lib.check(L.ckd_set_tuning(7, 0))
+        _lib.check(L.ckd_set_tuning(7, 1))
