@@ -663,7 +663,7 @@ def main():
     # Inside the NFW cusps a query holds up to ~10^5 neighbours within r, so the
     # full result (about 10^12 ids) cannot be materialised: the count pass (phase 1
     # of the CSR protocol) runs over every query, the full count + scan + fill over
-    # a random subset whose CSR fits in 2 GB.
+    # a random subset whose CSR holds about 1.5e9 results (24 GB).
     radius = 0.5 * n ** (-1.0 / 3.0)
     counts = torch.empty(nq, dtype=torch.int64, device="cuda")
     cp = ctypes.c_void_p(counts.data_ptr())
@@ -674,7 +674,7 @@ def main():
     ball_count_total, _, _ = timed(ball_count_step, args.steps, args.warmup)
     total_hits = int(counts.sum().item())
     mean_hits = total_hits / nq
-    m_ball = int(min(nq, max(1024, 1.2e8 / max(mean_hits, 1.0))))
+    m_ball = int(min(nq, max(1024, 1.5e9 / max(mean_hits, 1.0))))
     bq = Q[torch.randperm(nq, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))[:m_ball]].contiguous()
     bqp = ctypes.c_void_p(bq.data_ptr())
     bcounts = torch.empty(m_ball, dtype=torch.int64, device="cuda")

@@ -28,7 +28,8 @@ constexpr int kStack = 96;
 
 template <int D, bool PER, bool FILL>
 __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restrict__ Q,
-                                              const int32_t* __restrict__ order, int64_t nq,
+                                              const int32_t* __restrict__ order, int64_t nq_max,
+                                              const unsigned* __restrict__ nq_dev,
                                               double r2, int32_t* __restrict__ gstack,
                                               int stack_len, int64_t* __restrict__ counts,
                                               const int64_t* __restrict__ offsets,
@@ -38,6 +39,8 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int64_t gw = (int64_t)blockIdx.x * nw + w;
   int32_t* stk = gstack ? gstack + gw * stack_len : sstk[w];
+  const int64_t nq = nq_dev ? (int64_t)*nq_dev : nq_max;
+  if (gw * 32 >= nq) return;  // whole warp past the (device-side) query count
   int64_t slot = gw * 32 + lane;
   bool valid = slot < nq;
   int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
@@ -145,6 +148,117 @@ __global__ void k_sort_rows(const int64_t* __restrict__ offsets, int64_t nq,
     }
   }
   for (int64_t i = 0; i < n; ++i) D2[i] = sqrt(D2[i]);
+}
+
+// ---------------------------------------------------------- heavy ball rows
+// Rows with at least kHeavyRow results are filled by a whole warp per query:
+// one warp-uniform left-first DFS (stack in shared memory), leaves scanned with
+// the lanes over the points (FP64 distances, results compacted in point order by
+// ballot prefix), and subtrees whose tight box lies entirely inside the ball
+// (box_maxd2 / box_maxd2_near <= r^2) emitted in one coalesced pass over their
+// contiguous positions.  The order of a row is the per-lane kernel's: left-first
+// DFS, leaf order.
+constexpr int64_t kHeavyRow = 256;
+constexpr int kHeavyStack = 128;
+
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const double* __restrict__ Q,
+                                                        const int32_t* __restrict__ rows,
+                                                        const unsigned* __restrict__ n_rows,
+                                                        double r2, int32_t* __restrict__ gstack,
+                                                        int stack_len,
+                                                        const int64_t* __restrict__ offsets,
+                                                        int64_t* __restrict__ oidx,
+                                                        double* __restrict__ odist, int want_d2) {
+  __shared__ int32_t sstk[4][kHeavyStack];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int64_t nrows = (int64_t)*n_rows;
+  for (int64_t r = (int64_t)blockIdx.x * nw + w; r < nrows; r += (int64_t)gridDim.x * nw) {
+    int32_t* stk = gstack ? gstack + ((int64_t)blockIdx.x * nw + w) * stack_len : sstk[w];
+    const int64_t qi = rows[r];
+    double q[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) q[j] = Q[qi * D + j];
+    int64_t cur = offsets[qi];
+    const int64_t cur_end = offsets[qi + 1];
+    int top = 0;
+    if (lane == 0) stk[0] = 0;
+    __syncwarp();
+    while (top >= 0) {
+      const int32_t node = stk[top];
+      --top;
+      __syncwarp();
+      const NodeMeta m = load_meta(tv.meta, node);
+      if (!(box_mind2<D, PER>(tv, q, node) <= r2)) continue;
+      const bool inside =
+          m.left >= 0 && (PER ? box_maxd2_near<D>(tv, q, node) : box_maxd2<D>(tv, q, node)) <= r2;
+      if (inside) {  // whole subtree: positions m.start .. m.start + count - 1 in order
+        for (int32_t i = lane; i < m.count; i += 32) {
+          const int32_t p = m.start + i;
+          const int64_t o = cur + i;
+          if (o < cur_end) {
+            const double d2 = point_d2<D, PER>(tv, q, p);
+            oidx[o] = __ldg(&tv.ids[p]);
+            odist[o] = want_d2 ? d2 : sqrt(d2);
+          }
+        }
+        cur += m.count;
+      } else if (m.left < 0) {
+        for (int32_t base = 0; base < m.count; base += 32) {
+          const int32_t i = base + lane;
+          bool hit = false;
+          double d2 = 0.0;
+          if (i < m.count) {
+            d2 = point_d2<D, PER>(tv, q, m.start + i);
+            hit = d2 <= r2;
+          }
+          const unsigned hm = __ballot_sync(0xffffffffu, hit);
+          if (hit) {
+            const int64_t o = cur + __popc(hm & lt_mask);
+            if (o < cur_end) {
+              oidx[o] = __ldg(&tv.ids[m.start + i]);
+              odist[o] = want_d2 ? d2 : sqrt(d2);
+            }
+          }
+          cur += __popc(hm);
+        }
+      } else {
+        if (lane == 0) {
+          stk[top + 1] = m.left + 1;
+          stk[top + 2] = m.left;
+        }
+        top += 2;
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// rows of the fill split by length: heavy ones (>= kHeavyRow) to `heavy`, the rest
+// to `light`, both in the processing order (`order`, the leaf order when given)
+__global__ void k_split_rows(const int64_t* __restrict__ offsets, const int32_t* __restrict__ order,
+                             int64_t nq, int32_t* __restrict__ heavy,
+                             unsigned* __restrict__ n_heavy, int32_t* __restrict__ light,
+                             unsigned* __restrict__ n_light) {
+  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool valid = slot < nq;
+  const int64_t i = valid ? (order ? (int64_t)order[slot] : slot) : 0;
+  const bool h = valid && offsets[i + 1] - offsets[i] >= kHeavyRow;
+  const unsigned hm = __ballot_sync(0xffffffffu, h);
+  const unsigned lm = __ballot_sync(0xffffffffu, valid && !h);
+  unsigned hb = 0, lb = 0;
+  if (lane == 0) {
+    if (hm) hb = atomicAdd(n_heavy, (unsigned)__popc(hm));
+    if (lm) lb = atomicAdd(n_light, (unsigned)__popc(lm));
+  }
+  hb = __shfl_sync(0xffffffffu, hb, 0);
+  lb = __shfl_sync(0xffffffffu, lb, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (h) heavy[hb + __popc(hm & below)] = (int32_t)i;
+  if (valid && !h) light[lb + __popc(lm & below)] = (int32_t)i;
 }
 
 template <int D, bool FILL>
@@ -259,13 +373,38 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
   if (stack_len > kStack)
     CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
   double r2 = r * r;  // radius**2 (cosmokdtree.f90:1112)
-  if (fill)
-    k_ball<D, PER, true><<<blocks, threads, 0, s>>>(tv, q, order, nq, r2, gstack, stack_len,
-                                                     nullptr, offsets, idx, dist, sorted ? 1 : 0);
-  else
-    k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, r2, gstack, stack_len,
-                                                      counts, nullptr, nullptr, nullptr, 0);
-  CKD_LAUNCH_CHECK();
+  if (fill) {
+    // heavy rows: a warp per query; light rows: the per-lane kernel over a list
+    int32_t *heavy = nullptr, *light = nullptr, *hstack = nullptr;
+    unsigned* cnt = nullptr;
+    CKD_CUDA(dev_alloc((void**)&heavy, sizeof(int32_t) * nq, s));
+    CKD_CUDA(dev_alloc((void**)&light, sizeof(int32_t) * nq, s));
+    CKD_CUDA(dev_alloc((void**)&cnt, 2 * sizeof(unsigned), s));
+    CKD_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s));
+    k_split_rows<<<(unsigned)cdiv(nq, 256), 256, 0, s>>>(offsets, order, nq, heavy, cnt, light,
+                                                         cnt + 1);
+    CKD_LAUNCH_CHECK();
+    k_ball<D, PER, true><<<blocks, threads, 0, s>>>(tv, q, light, nq, cnt + 1, r2, gstack,
+                                                     stack_len, nullptr, offsets, idx, dist,
+                                                     sorted ? 1 : 0);
+    CKD_LAUNCH_CHECK();
+    int dev = 0, sms = 148;
+    CKD_CUDA(cudaGetDevice(&dev));
+    CKD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t hblocks = std::min<int64_t>(cdiv(nq, 4), (int64_t)sms * 8);
+    const int hstack_len = std::max(kHeavyStack, t->depth + 4);
+    if (hstack_len > kHeavyStack)
+      CKD_CUDA(dev_alloc((void**)&hstack, sizeof(int32_t) * hstack_len * hblocks * 4, s));
+    k_ball_fill_warp<D, PER><<<(unsigned)std::max<int64_t>(1, hblocks), 128, 0, s>>>(
+        tv, q, heavy, cnt, r2, hstack, hstack_len, offsets, idx, dist, sorted ? 1 : 0);
+    CKD_LAUNCH_CHECK();
+    for (void* p : {(void*)heavy, (void*)light, (void*)cnt, (void*)hstack}) dev_free(p, s);
+  } else {
+    k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2, gstack,
+                                                      stack_len, counts, nullptr, nullptr, nullptr,
+                                                      0);
+    CKD_LAUNCH_CHECK();
+  }
   if (fill && sorted) {
     k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist);
     CKD_LAUNCH_CHECK();
