@@ -150,6 +150,7 @@ static void release_tree(ckd_tree* t) {
   cudaFree(t->ids);
   cudaFree(t->box32);
   cudaFree(t->pts32);
+  cudaFree(t->pts64);
   cudaFree(t->pair);
   cudaFree(t->cell32);
   cudaFree(t->centre);

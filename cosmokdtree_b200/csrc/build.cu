@@ -487,6 +487,20 @@ __global__ void k_box32(const double* __restrict__ box, int32_t n_nodes, float* 
   box32[i] = (i & 1) ? __double2float_ru(v) : __double2float_rd(v);
 }
 
+// FP64 points as packed records of (d + 3) / 4 double4s (zero padded)
+template <int D>
+__global__ void k_pts64(const double* __restrict__ Pf, int64_t n, double4* __restrict__ P64) {
+  constexpr int NV = (D + 3) / 4;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double v[4 * NV];
+#pragma unroll
+  for (int j = 0; j < 4 * NV; ++j) v[j] = j < D ? Pf[(int64_t)(j < D ? j : 0) * n + p] : 0.0;
+#pragma unroll
+  for (int h = 0; h < NV; ++h)
+    P64[p * NV + h] = make_double4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+}
+
 // Each point relative to its leaf's box centre, rounded to FP32, packed in float4s.
 template <int D>
 __global__ void k_pts32(const NodeMeta* __restrict__ meta, int32_t n_nodes, int leaf,
@@ -825,6 +839,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   constexpr int NV = (D + 3) / 4;
   CKD_CUDA(cudaMalloc((void**)&t->box32, sizeof(float) * 2 * D * n_nodes));
   CKD_CUDA(cudaMalloc((void**)&t->pts32, sizeof(float4) * NV * n));
+  CKD_CUDA(cudaMalloc((void**)&t->pts64, sizeof(double4) * NV * n));
+  k_pts64<D><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(t->pts, n, t->pts64);
+  CKD_LAUNCH_CHECK();
   k_box32<D><<<(unsigned)cdiv((int64_t)n_nodes * 2 * D, 256), 256, 0, s>>>(t->box, n_nodes, t->box32);
   CKD_LAUNCH_CHECK();
   k_pts32<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(t->meta, n_nodes, leaf, t->box, t->pts, n,

@@ -92,6 +92,9 @@ struct TreeView {
   // each point relative to its leaf's box centre, 1 (d <= 4) or 2 float4 per point
   const float* box32;        // [n_nodes][2d]
   const float4* pts32;       // [n][(d + 3) / 4]
+  // the FP64 points again, one 32-byte (d <= 4) or 64-byte record per point, so an
+  // exact distance evaluation touches one or two sectors instead of d
+  const double4* pts64;      // [n][(d + 3) / 4]
   float slack[CKD_MAX_D];    // per-axis absolute slack of FP32 node-box gaps
   // bottom-up search records
   const float4* pair;        // per internal node: both children's FP32 boxes + ids/flags
@@ -195,6 +198,7 @@ struct ckd_tree {
   int32_t* ids = nullptr;
   float* box32 = nullptr;
   float4* pts32 = nullptr;
+  double4* pts64 = nullptr;
   float slack[CKD_MAX_D] = {0};
   bool screen_ok = false;  // FP32 screen usable (coordinates well inside FP32 range)
   float4* pair = nullptr;
@@ -214,6 +218,7 @@ struct ckd_tree {
     v.ids = ids;
     v.box32 = box32;
     v.pts32 = pts32;
+    v.pts64 = pts64;
     for (int j = 0; j < CKD_MAX_D; ++j) v.slack[j] = slack[j];
     v.pair = pair;
     v.cell32 = cell32;

@@ -20,6 +20,30 @@ __device__ __forceinline__ double point_d2(const TreeView& tv, const double (&q)
   return s;
 }
 
+// point_d2 from the packed FP64 records (same operations, same result)
+template <int D, bool PER>
+__device__ __forceinline__ double point_d2_rec(const TreeView& tv, const double (&q)[D], int32_t p) {
+  constexpr int NV = (D + 3) / 4;
+  double v[4 * NV];
+#pragma unroll
+  for (int h = 0; h < NV; ++h) {
+    const double2* r = reinterpret_cast<const double2*>(tv.pts64 + (int64_t)p * NV + h);
+    const double2 a = __ldg(r), b = __ldg(r + 1);
+    v[4 * h] = a.x;
+    v[4 * h + 1] = a.y;
+    v[4 * h + 2] = b.x;
+    v[4 * h + 3] = b.y;
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    double dx = dsub(v[j], q[j]);
+    if (PER) dx = min_image(dx, tv.L[j]);
+    s = (j == 0) ? dmul(dx, dx) : dadd(s, dmul(dx, dx));
+  }
+  return s;
+}
+
 // Conservative lower bound of the squared distance from q to any point of the
 // node's tight bounding box.
 template <int D, bool PER>

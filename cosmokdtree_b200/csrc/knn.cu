@@ -875,7 +875,7 @@ struct CompactCtx {
   const double (&q)[D];
   double rr;  // bounded sentinel's squared distance
   __device__ __forceinline__ double exact(int32_t p) const {
-    return p >= 0 ? point_d2<D, PER>(tv, q, p) : (p == kPosMissing ? CKD_HUGE : rr);
+    return p >= 0 ? point_d2_rec<D, PER>(tv, q, p) : (p == kPosMissing ? CKD_HUGE : rr);
   }
   __device__ __forceinline__ int32_t id(int32_t p) const {
     return p >= 0 ? __ldg(&tv.ids[p]) : (p == kPosMissing ? -1 : 0x7fffffff);
@@ -1050,6 +1050,11 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
       st[3] += m.count;
     }
     float qr[D], e[D];
+    // near: on every axis the whole leaf lies within half a box side of the
+    // query's image, so the minimum image of each point difference is the
+    // direct difference and the screen skips the wrap (exactly: every |v - qr|
+    // stays below L/2 even after rounding)
+    bool near = true;
     {
       const double* b = tv.box + (int64_t)node * 2 * D;
 #pragma unroll
@@ -1062,6 +1067,7 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
           double h = 0.5 * tv.L[j];
           if (x > h) x -= tv.L[j];
           else if (x < -h) x += tv.L[j];
+          near = near && fabs(x) + r < 0.49 * tv.L[j];
         }
         qr[j] = __double2float_rn(x);
         e[j] = kTwoM21 * (float)(r + fabs(x) + (PER ? tv.L[j] : 0.0)) * 1.0001f + 1e-37f;
@@ -1071,32 +1077,53 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
       const int cnt = min(32, m.count - base);
       const int32_t p0 = m.start + base;
       unsigned mask = 0;
-      for (int i = 0; i < cnt; ++i) {
-        float v[4 * NV];
+      if (!PER || near) {
+        for (int i = 0; i < cnt; ++i) {
+          float v[4 * NV];
 #pragma unroll
-        for (int h = 0; h < NV; ++h) {
-          float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
-          v[4 * h] = f.x;
-          v[4 * h + 1] = f.y;
-          v[4 * h + 2] = f.z;
-          v[4 * h + 3] = f.w;
-        }
-        float s = 0.0f;
+          for (int h = 0; h < NV; ++h) {
+            float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+            v[4 * h] = f.x;
+            v[4 * h + 1] = f.y;
+            v[4 * h + 2] = f.z;
+            v[4 * h + 3] = f.w;
+          }
+          float s = 0.0f;
 #pragma unroll
-        for (int j = 0; j < D; ++j) {
-          float a = fabsf(v[j] - qr[j]);
-          if (PER) a = fminf(a, (float)tv.L[j] - a);
-          a = fmaxf(a - e[j], 0.0f);
-          s = fmaf(a, a, s);
+          for (int j = 0; j < D; ++j) {
+            float a = fmaxf(fabsf(v[j] - qr[j]) - e[j], 0.0f);
+            s = fmaf(a, a, s);
+          }
+          if (s * kShrink <= wd32) mask |= 1u << i;
         }
-        if (s * kShrink <= wd32) mask |= 1u << i;
+      } else {
+        for (int i = 0; i < cnt; ++i) {
+          float v[4 * NV];
+#pragma unroll
+          for (int h = 0; h < NV; ++h) {
+            float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
+            v[4 * h] = f.x;
+            v[4 * h + 1] = f.y;
+            v[4 * h + 2] = f.z;
+            v[4 * h + 3] = f.w;
+          }
+          float s = 0.0f;
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            float a = fabsf(v[j] - qr[j]);
+            a = fminf(a, (float)tv.L[j] - a);
+            a = fmaxf(a - e[j], 0.0f);
+            s = fmaf(a, a, s);
+          }
+          if (s * kShrink <= wd32) mask |= 1u << i;
+        }
       }
       if (stats) st[5] += __popc(mask);
       while (mask) {
         const int i = __ffs(mask) - 1;
         mask &= mask - 1;
         const int32_t p = p0 + i;
-        const double d2 = point_d2<D, PER>(tv, q, p);
+        const double d2 = point_d2_rec<D, PER>(tv, q, p);
         const unsigned kc = __float_as_uint(__double2float_rn(d2));
         if (kc > wk) continue;
         if (kc == wk) {  // FP32 tie with the root: exact comparison
@@ -1214,7 +1241,7 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
       double d2 = CKD_HUGE;
       int64_t id = -2;
       if (p >= 0) {
-        d2 = point_d2<D, PER>(tv, qx, p);
+        d2 = point_d2_rec<D, PER>(tv, qx, p);
         id = (int64_t)__ldg(&tv.ids[p]);
       }
       dist[row * k + j] = sqrt(d2);
