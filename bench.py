@@ -326,6 +326,96 @@ def run_forest(args):
     return 0
 
 
+def run_small_uniform(args):
+    """The reference's small configuration: 2^20 uniform points in [0,1)^3, non-periodic,
+    leaf 16; 10^5 uniform queries: kNN k=16 sorted, ball r=0.01 sorted (CSR), 10^3 boxes
+    of side 0.02 at uniform centres; seed 0.  GPU times with CUDA events (inputs on the
+    device), the CPU oracle on all host cores for the same calls, results compared."""
+    import torch
+    import oracle
+    from cosmokdtree_b200 import _lib, kdtree
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L = _lib.load()
+    rng = np.random.default_rng(0)
+    P = rng.random((1 << 20, 3))
+    Qh = rng.random((100_000, 3))
+    cen = rng.random((1000, 3))
+    B = np.empty((1000, 6))
+    B[:, 0::2] = cen - 0.01
+    B[:, 1::2] = cen + 0.01
+    Pd, Qd, Bd = (torch.from_numpy(x).cuda() for x in (P, Qh, B))
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    holder = {}
+
+    def build():
+        if "t" in holder:
+            holder["t"].close()
+        holder["t"] = kdtree.build_kdtree(Pd, leaf=16)
+        return holder["t"]
+
+    l0 = L.ckd_launch_count()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        build_ms, t = timed(build)
+        knn_ms, (kd, ki) = timed(lambda: kdtree.knn_search_batch(t, Qd, 16, sorted=True))
+        ball_ms, (bo, bi, bd) = timed(lambda: kdtree.ball_search_csr(t, Qd, 0.01, sorted=True))
+        box_ms, (xo, xi) = timed(lambda: kdtree.box_search_csr(t, Bd))
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ot = oracle.OracleTree(P, 16, None, threads=threads)
+    cpu_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    od, oi = ot.knn(Qh, 16)
+    cpu_knn = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oo, ob, obd = ot.ball_csr(Qh, 0.01, sorted=True)
+    cpu_ball = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    xo_o, xi_o = ot.box_csr(B)
+    cpu_box = time.perf_counter() - t0
+    exact = (np.array_equal(ki.cpu().numpy(), oi) and np.array_equal(kd.cpu().numpy(), od) and
+             np.array_equal(bo.cpu().numpy(), oo) and np.array_equal(bi.cpu().numpy(), ob) and
+             np.array_equal(bd.cpu().numpy(), obd) and np.array_equal(xo.cpu().numpy(), xo_o) and
+             np.array_equal(xi.cpu().numpy(), xi_o))
+    nq = len(Qh)
+    out = {
+        "metric": "knn_queries_per_s", "value": nq / (knn_ms / 1e3), "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": knn_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "uniform_2p20_small", "n_points": 1 << 20, "n_queries": nq, "k": 16,
+                   "ball_radius": 0.01, "boxes": 1000, "box_side": 0.02, "periodic": False,
+                   "leaf": 16, "seed": 0, "l2": "tree and queries fit in L2 (small configuration)"},
+        "knn": {"gpu_ms": knn_ms, "cpu_ms": cpu_knn * 1e3, "speedup": cpu_knn * 1e3 / knn_ms},
+        "ball": {"gpu_ms": ball_ms, "cpu_ms": cpu_ball * 1e3, "speedup": cpu_ball * 1e3 / ball_ms,
+                 "hits": int(bo[-1].item()), "sorted": True},
+        "box": {"gpu_ms": box_ms, "cpu_ms": cpu_box * 1e3, "speedup": cpu_box * 1e3 / box_ms,
+                "hits": int(xo[-1].item())},
+        "build": {"gpu_ms": build_ms, "cpu_ms": cpu_build * 1e3,
+                  "mpts_per_s": (1 << 20) / (build_ms / 1e3) / 1e6},
+        "cpu_baseline": {"value": nq / cpu_knn, "unit": "queries/s", "cores": threads,
+                         "kind": "port", "sample": "the full configuration (10^5 queries)"},
+        "gpu_launches": int(L.ckd_launch_count() - l0),
+        "clocks": clk.summary(),
+        "exact_vs_oracle": bool(exact),
+    }
+    print(json.dumps(out))
+    t.close()
+    return 0
+
+
 def run_multi(args):
     """Learned-bound vs plain kNN on a configuration with its own queries: several k
     (queries split evenly, one search call per k), optional 6-D float32 input.  The
@@ -491,7 +581,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     choices=sorted(WORKLOADS) + sorted(FOREST_WORKLOADS) +
-                    sorted(MULTI_WORKLOADS))
+                    sorted(MULTI_WORKLOADS) + ["uniform_2p20_small"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -502,7 +592,8 @@ def main():
                     help="one build and the kNN steps only (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
-        if args.workload in FOREST_WORKLOADS or args.workload in MULTI_WORKLOADS:
+        if args.workload in FOREST_WORKLOADS or args.workload in MULTI_WORKLOADS or \
+                args.workload == "uniform_2p20_small":
             print(json.dumps({"impl": "reference", "unavailable": "this workload's CPU "
                               "baseline is reported inside the ours line (sampled queries)"}))
             return 0
@@ -511,6 +602,8 @@ def main():
         return run_forest(args)
     if args.workload in MULTI_WORKLOADS:
         return run_multi(args)
+    if args.workload == "uniform_2p20_small":
+        return run_small_uniform(args)
 
     import torch
     import torch.distributed as dist

@@ -261,6 +261,67 @@ __global__ void k_split_rows(const int64_t* __restrict__ offsets, const int32_t*
   if (valid && !h) light[lb + __popc(lm & below)] = (int32_t)i;
 }
 
+// Per-lane box search: each lane walks the tree for its own box with a private
+// stack, left child first, so a row comes out in the same order as the packet
+// kernel below (left-first DFS, leaf order) without the warp serialising the union
+// of 32 boxes' paths.  Stack depth <= tree depth + 1 (<= 2 pushes per pop).
+constexpr int kBoxLaneStack = 128;
+
+template <int D, bool FILL>
+__global__ void __launch_bounds__(128) k_box_lane(TreeView tv, const double* __restrict__ boxes,
+                                                  int64_t nb, int64_t* __restrict__ counts,
+                                                  const int64_t* __restrict__ offsets,
+                                                  int64_t* __restrict__ oidx,
+                                                  const int32_t* __restrict__ broot) {
+  const int64_t bi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (bi >= nb) return;
+  double lo[D], hi[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    lo[j] = boxes[bi * 2 * D + 2 * j];
+    hi[j] = boxes[bi * 2 * D + 2 * j + 1];
+  }
+  int64_t cnt = 0;
+  int64_t cur = FILL ? offsets[bi] : 0;
+  const int64_t cur_end = FILL ? offsets[bi + 1] : 0;
+  int32_t stk[kBoxLaneStack];
+  int top = 0;
+  stk[0] = broot ? broot[bi] : 0;
+  while (top >= 0) {
+    const int32_t node = stk[top--];
+    const NodeMeta m = load_meta(tv.meta, node);
+    if (m.left < 0) {
+      for (int i = 0; i < m.count; ++i) {
+        const int32_t p = m.start + i;
+        bool in = true;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          const double x = __ldg(&tv.pts[(int64_t)j * tv.n + p]);
+          in = in && !(x < lo[j] || x > hi[j]);  // :1319
+        }
+        if (in) {
+          if (FILL) {
+            if (cur < cur_end) oidx[cur++] = __ldg(&tv.ids[p]);
+          } else {
+            ++cnt;
+          }
+        }
+      }
+    } else {
+      double bl = 0.0, bh = 0.0;
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        if (j == m.axis) {
+          bl = lo[j];
+          bh = hi[j];
+        }
+      if (bh > m.split) stk[++top] = m.left + 1;  // :1300 (visited second)
+      if (bl < m.split) stk[++top] = m.left;      // :1296 (visited first)
+    }
+  }
+  if (!FILL) counts[bi] = cnt;
+}
+
 template <int D, bool FILL>
 __global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restrict__ boxes,
                                              int64_t nb, int32_t* __restrict__ gstack,
@@ -419,6 +480,15 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
                       const int32_t* broot) {
   TreeView tv = t->view();
   const int threads = 128, nw = threads / 32;
+  if (t->depth < kBoxLaneStack - 2) {
+    const unsigned lb = (unsigned)cdiv(nb, threads);
+    if (fill)
+      k_box_lane<D, true><<<lb, threads, 0, s>>>(tv, boxes, nb, nullptr, offsets, idx, broot);
+    else
+      k_box_lane<D, false><<<lb, threads, 0, s>>>(tv, boxes, nb, counts, nullptr, nullptr, broot);
+    CKD_LAUNCH_CHECK();
+    return CKD_OK;
+  }
   int64_t warps = cdiv(nb, 32);
   unsigned blocks = (unsigned)cdiv(warps, nw);
   // a packet stack grows by at most one entry per level past its start entries
