@@ -36,13 +36,13 @@ _KEY_VARIANT, _KEY_BPS, _KEY_WPB, _KEY_ORDER = 0, 1, 2, 6
 
 DEFAULT_GRID = {
     "leaf": (8, 16, 32),
-    "variant": (3, 2, 4, 6),
-    "warps_per_block": (2, 4, 8),
+    "variant": (7, 8, 3, 2),
+    "warps_per_block": (1, 2, 4),
     "blocks_per_sm": (0,),
     "order": (0,),
 }
 
-DEFAULT_CONFIG = {"leaf": 16, "variant": 0, "warps_per_block": 4, "blocks_per_sm": 0, "order": 0}
+DEFAULT_CONFIG = {"leaf": 16, "variant": 0, "warps_per_block": 2, "blocks_per_sm": 0, "order": 0}
 
 
 def config_key(d: int, k: int, dtype: str, periodic: bool, n: int, device_name: str) -> str:
