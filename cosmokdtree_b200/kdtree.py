@@ -32,7 +32,7 @@ from ._lib import CKDArgumentError, check
 
 __all__ = [
     "KDTree", "build_kdtree", "deallocate_kdtree", "knn_search", "ball_search", "box_search",
-    "knn_search_batch", "ball_search_csr", "box_search_csr",
+    "knn_search_batch", "ball_search_csr", "box_search_csr", "box_search_periodic_csr",
 ]
 
 
@@ -299,3 +299,61 @@ def box_search(tree: KDTree, box):
     offsets, idx = box_search_csr(tree, b.reshape(1, -1))
     with torch.cuda.device(tree.device):
         return _to_host(idx)
+
+
+def _wrap_pieces(lo, hi, L):
+    """Pieces of [lo, hi] on a periodic axis of side L, each inside [-L/2, L/2]."""
+    if hi - lo >= L:
+        return [(-L / 2, L / 2)]
+    a = ((lo + L / 2) % L) - L / 2
+    b = a + (hi - lo)
+    if b <= L / 2:
+        return [(a, b)]
+    return [(a, L / 2), (-L / 2, b - L)]
+
+
+def box_search_periodic_csr(tree: KDTree, boxes):
+    """Box search that wraps boxes across the faces of a periodic tree (opt-in).
+
+    The reference's box_search never wraps (src/cosmokdtree.f90:1258-1328): a box
+    that crosses a face of the periodic box silently misses the points on the far
+    side, and ``box_search`` / ``box_search_csr`` keep that behaviour.  Here each box
+    [lo0, hi0, lo1, hi1, ...] (coordinates in any image; a side >= L covers the whole
+    axis) is split on every axis into at most two pieces inside [-L/2, L/2], the
+    pieces are searched with the reference's descent rule, and each box's ids are
+    returned sorted.  Returns CSR CUDA tensors (offsets (nb+1,), idx)."""
+    if not tree.periodic:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "periodic box search needs a periodic tree")
+    b = boxes.detach().cpu().numpy() if _on_device(boxes) else np.asarray(boxes, dtype=np.float64)
+    b = np.array(b, dtype=np.float64, ndmin=2)
+    d = tree.d
+    if b.shape[-1] != 2 * d:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
+                               "Error: box size does not match tree dimensionality.")
+    if not np.all(np.isfinite(b)):
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "box coordinates must be finite")
+    L = tree.boxsize
+    pieces, owner = [], []
+    for i, row in enumerate(b):
+        axes = [_wrap_pieces(row[2 * j], row[2 * j + 1], L[j]) for j in range(d)]
+        combos = [[]]
+        for ax in axes:
+            combos = [c + [p] for c in combos for p in ax]
+        for c in combos:
+            pieces.append([v for lohi in c for v in lohi])
+            owner.append(i)
+    nb = b.shape[0]
+    with torch.cuda.device(tree.device):
+        if not pieces:
+            return (torch.zeros(nb + 1, dtype=torch.int64, device=f"cuda:{tree.device}"),
+                    torch.empty(0, dtype=torch.int64, device=f"cuda:{tree.device}"))
+        off, idx = box_search_csr(tree, np.array(pieces))
+        dev = off.device
+        own = torch.as_tensor(owner, dtype=torch.int64, device=dev)
+        rows = torch.repeat_interleave(own, off[1:] - off[:-1])
+        key = torch.unique(rows * max(1, tree.n) + idx)  # sorted; drops repeats
+        rows, idx = key // max(1, tree.n), key % max(1, tree.n)
+        counts = torch.bincount(rows, minlength=nb)
+        offsets = torch.zeros(nb + 1, dtype=torch.int64, device=dev)
+        offsets[1:] = torch.cumsum(counts, 0)
+    return offsets, idx

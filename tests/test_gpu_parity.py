@@ -269,3 +269,30 @@ def test_gpu_errors_and_recovery(gpu):
     kd.deallocate_kdtree(t)
     with pytest.raises(AssertionError):
         kd.knn_search(t, P[:3], 4)
+
+
+def test_gpu_periodic_box_wraps(gpu):
+    """Opt-in wrapped box search on a periodic tree: every point whose minimum-image
+    offset from the box's low corner lies within the box's sides, for boxes that
+    cross faces, lie in other images or span whole axes."""
+    kd = gpu.kdtree
+    rng = np.random.default_rng(71)
+    P = rng.random((30000, 3)) - 0.5
+    t = kd.build_kdtree(P, leaf=16, boxsize=1.0)
+    lo = rng.random((40, 3)) * 2.0 - 1.0          # any image
+    side = 0.05 + 0.3 * rng.random((40, 3))
+    side[0] = [1.2, 0.1, 0.1]                      # whole first axis
+    B = np.empty((40, 6))
+    B[:, 0::2] = lo
+    B[:, 1::2] = lo + side
+    off, idx = (x.cpu().numpy() for x in kd.box_search_periodic_csr(t, B))
+    for r in range(40):
+        dlt = np.mod(P - lo[r], 1.0)
+        inside = np.all((dlt <= side[r]) | (side[r] >= 1.0), axis=1)
+        np.testing.assert_array_equal(idx[off[r]:off[r + 1]], np.nonzero(inside)[0])
+    # boxes inside the box give the reference's (non-wrapping) answer as a set
+    inner = np.array([[-0.2, 0.1, -0.05, 0.2, -0.1, 0.1]])
+    o2, i2 = (x.cpu().numpy() for x in kd.box_search_periodic_csr(t, inner))
+    np.testing.assert_array_equal(i2, np.sort(kd.box_search(t, inner[0])))
+    with pytest.raises(AssertionError):
+        kd.box_search_periodic_csr(kd.build_kdtree(P), inner)
