@@ -92,6 +92,8 @@ SIGNATURES = {
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],
     "ckd_box_fill": [_vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_exclusive_scan": [_vp, _vp, _i64, _vp],
+    "ckd_tree_save": [_vp, ctypes.c_char_p],
+    "ckd_tree_load": [ctypes.c_char_p, ctypes.POINTER(_vp)],
     "ckd_forest_build": [_vp, _pi64, _i64, _int, _int, _int, _pdbl, _int, _vp,
                          ctypes.POINTER(_vp)],
     "ckd_forest_info": [_vp, _pi64, _pi64],

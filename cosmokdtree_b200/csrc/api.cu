@@ -157,6 +157,8 @@ static void release_tree(ckd_tree* t) {
   delete t;
 }
 
+void release_tree_handle(ckd_tree* t) { release_tree(t); }
+
 }  // namespace ckd
 
 using namespace ckd;

@@ -23,6 +23,7 @@ reference returns them.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -33,6 +34,7 @@ from ._lib import CKDArgumentError, check
 __all__ = [
     "KDTree", "build_kdtree", "deallocate_kdtree", "knn_search", "ball_search", "box_search",
     "knn_search_batch", "ball_search_csr", "box_search_csr", "box_search_periodic_csr",
+    "save_kdtree", "load_kdtree", "read_fortran_points",
 ]
 
 
@@ -357,3 +359,70 @@ def box_search_periodic_csr(tree: KDTree, boxes):
         offsets = torch.zeros(nb + 1, dtype=torch.int64, device=dev)
         offsets[1:] = torch.cumsum(counts, 0)
     return offsets, idx
+
+
+# ---------------------------------------------------------------- files
+
+def save_kdtree(tree, path: str) -> None:
+    """Write a built tree (or forest) to ``path``; ``load_kdtree`` restores it without
+    rebuilding and with bit-identical results."""
+    with torch.cuda.device(tree.device):
+        check(_lib.load().ckd_tree_save(tree.handle, os.fsencode(path)))
+
+
+def load_kdtree(path: str, device=None):
+    """Load a tree saved by ``save_kdtree`` onto ``device`` (default: current).
+    Returns a KDTree, or a Forest when the file holds several trees."""
+    device = torch.cuda.current_device() if device is None else int(device)
+    L = _lib.load()
+    with torch.cuda.device(device):
+        h = ctypes.c_void_p()
+        check(L.ckd_tree_load(os.fsencode(path), ctypes.byref(h)))
+        n, d, leaf, per = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(L.ckd_tree_info(h, ctypes.byref(n), ctypes.byref(d), ctypes.byref(leaf),
+                              ctypes.byref(per), None, None, None, None))
+        nt = ctypes.c_int64()
+        check(L.ckd_forest_info(h, ctypes.byref(nt), None))
+        off = np.empty(nt.value + 1, np.int64)
+        check(L.ckd_forest_info(h, None, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        box = None
+        if per.value:
+            box = _saved_boxsize(path, d.value)
+    if nt.value > 1:
+        from .forest import Forest
+        return Forest(h, off, d.value, leaf.value, box, device)
+    return KDTree(h, int(n.value), d.value, leaf.value, box, device)
+
+
+def _saved_boxsize(path: str, d: int) -> np.ndarray:
+    # header after the 8-byte magic: 2 int64, 8 int32, then 8 float64 box sides
+    with open(path, "rb") as f:
+        f.seek(8 + 16 + 32)
+        return np.frombuffer(f.read(8 * d), dtype=np.float64).copy()
+
+
+def read_fortran_points(path: str, dtype=np.float32) -> np.ndarray:
+    """Read a point file in the reference's Fortran unformatted sequential layout
+    (build/inhomogeneous/tree_test.f90:72-81, generate_inhomogeneous_distribution.py:61-65):
+    a record holding the int32 point count n, then one record per coordinate axis
+    holding n values (float32 by default).  Each record is framed by 4-byte length
+    markers.  Returns an (n, d) array (d = number of coordinate records)."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    pos, recs = 0, []
+    while pos < raw.size:
+        if pos + 4 > raw.size:
+            raise ValueError(f"{path}: truncated record marker")
+        ln = int(raw[pos:pos + 4].view(np.int32)[0])
+        body = raw[pos + 4:pos + 4 + ln]
+        end = pos + 4 + ln
+        if ln < 0 or end + 4 > raw.size or int(raw[end:end + 4].view(np.int32)[0]) != ln:
+            raise ValueError(f"{path}: inconsistent record markers")
+        recs.append(body)
+        pos = end + 4
+    if not recs or recs[0].size != 4:
+        raise ValueError(f"{path}: first record must hold the int32 point count")
+    n = int(recs[0].view(np.int32)[0])
+    axes = [r.view(dtype) for r in recs[1:]]
+    if not axes or any(a.size != n for a in axes):
+        raise ValueError(f"{path}: coordinate records must each hold {n} values")
+    return np.ascontiguousarray(np.stack(axes, axis=1))

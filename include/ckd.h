@@ -110,11 +110,12 @@ ckd_status ckd_set_knn_variant(int variant);
  * set by the autotuner).  key 0: kNN variant (as ckd_set_knn_variant);
  * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
  * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
- * of the kNN kernel (1..8, default 2; the per-lane kernels use at most 4); key 3: radius factor of the warp-per-bucket
- * kNN search in hundredths (default 150 = 1.5x the density estimate); key 4:
- * search kernel of ckd_knn_learned (0 = bounded per-lane traversal with 8-byte
- * heap entries; 1 = warp gather; 2 = bounded per-lane with 12-byte entries; 3 = 0
- * with child-pair-record descent, default); key 5: warps per block of the warp-gather kernel (1..4, default 2);
+ * of the kNN kernel (1..8, default 2; the per-lane kernels use at most 4); key 3:
+ * radius factor of the warp-per-bucket kNN search in hundredths (default 150 =
+ * 1.5x the density estimate); key 4: search kernel of ckd_knn_learned (0 = bounded
+ * per-lane traversal with 8-byte heap entries; 1 = warp gather; 2 = bounded
+ * per-lane with 12-byte entries; 3 = 0 with child-pair-record descent, default);
+ * key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
  * default; 1 = always; 2 = never); key 7: inference of the learned-bound network
  * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations, default). */
@@ -208,6 +209,13 @@ ckd_status ckd_forest_box_count(const ckd_tree* forest, const double* boxes_dev,
 ckd_status ckd_forest_box_fill(const ckd_tree* forest, const double* boxes_dev,
                                const int64_t* b_offsets_dev, int64_t nb,
                                const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
+
+/* Save a built tree or forest to a file / load it onto the current device (no
+ * counterpart in the reference, which rebuilds on every run).  The file is a raw
+ * copy of the handle's arrays, so a loaded tree gives bit-identical results.
+ * Synchronous. */
+ckd_status ckd_tree_save(const ckd_tree* tree, const char* path);
+ckd_status ckd_tree_load(const char* path, ckd_tree** out);
 
 /* out_dev[0] = 0, out_dev[i+1] = in_dev[0] + ... + in_dev[i]  (n+1 outputs). */
 ckd_status ckd_exclusive_scan(const int64_t* in_dev, int64_t* out_dev, int64_t n, void* stream);
