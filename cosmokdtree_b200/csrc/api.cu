@@ -141,19 +141,16 @@ static ckd_status check_tree(const ckd_tree* t) {
   return CKD_OK;
 }
 
+// Tree arrays come from the library's stream-ordered pool (a freed tree's memory
+// is reused by the next build without new device mappings).  Work that may still
+// read the tree ends first, as with cudaFree.
 static void release_tree(ckd_tree* t) {
   if (!t) return;
-  cudaFree(t->meta);
-  cudaFree(t->box);
-  cudaFree(t->cell);
-  cudaFree(t->pts);
-  cudaFree(t->ids);
-  cudaFree(t->box32);
-  cudaFree(t->pts32);
-  cudaFree(t->pts64);
-  cudaFree(t->pair);
-  cudaFree(t->cell32);
-  cudaFree(t->centre);
+  cudaDeviceSynchronize();
+  void* ps[] = {t->meta, t->box,   t->cell, t->pts,    t->ids,   t->box32,
+                t->pts32, t->pts64, t->pair, t->cell32, t->centre};
+  for (void* p : ps)
+    if (p) cudaFreeAsync(p, 0);
   delete t;
 }
 
@@ -312,6 +309,14 @@ ckd_status ckd_forest_box_count(const ckd_tree* t, const double* boxes, const in
 ckd_status ckd_forest_box_fill(const ckd_tree* t, const double* boxes, const int64_t* b_offsets,
                                int64_t nb, const int64_t* offsets, int64_t* idx, void* stream) {
   return forest_box(t, boxes, b_offsets, nb, true, nullptr, offsets, idx, stream);
+}
+
+ckd_status ckd_release_cached_memory(void) {
+  cudaMemPool_t pool;
+  CKD_CUDA(pool_for_current(&pool));
+  CKD_CUDA(cudaDeviceSynchronize());
+  CKD_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return CKD_OK;
 }
 
 ckd_status ckd_free(ckd_tree* tree) {

@@ -12,12 +12,16 @@
 //   k_scatter     stable out-of-place partition into the other buffer; points of
 //                 new leaves also land in the final leaf-ordered arrays
 //
-// Points live in SoA ping-pong buffers X[2][d][n]; each position carries the id
-// of the node whose segment holds it (NID).  A position is open at level L iff
-// its node has depth L and more than `leaf` points, so stale NIDs of finished
-// segments never need clearing.  The partition is stable, so every segment stays
-// sorted by original index and "first occurrence" (Fortran minloc/maxloc,
-// cosmokdtree.f90:372-373) is the lowest index holding the extreme.
+// The working set of a level holds only the points of open nodes (more than
+// `leaf` points), compacted into SoA ping-pong buffers X[2][d][n] (stride n):
+// open node a owns working positions [wst[a], wst[a] + count), in the order of
+// its final leaf-ordered range [start, start + count), and every position
+// carries its node's id (NID).  A point whose child is a leaf goes straight to
+// its final place in the leaf-ordered arrays and leaves the working set, so the
+// per-level passes touch only the points still being split.  The partition is
+// stable, so every segment stays sorted by original index and "first
+// occurrence" (Fortran minloc/maxloc, cosmokdtree.f90:372-373) is the lowest
+// index holding the extreme.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -53,16 +57,16 @@ struct BuildBufs {
   int32_t* pend = nullptr;             // local inclusive prefix at segment end
   int32_t* nleft = nullptr;
   int32_t* pbase = nullptr;
+  int32_t* wst = nullptr;              // first working position of an open node
   // per level
   int32_t* act[2] = {nullptr, nullptr};
   int32_t* nxt_cnt = nullptr;
   int32_t* nxt_off = nullptr;
+  int32_t* wcnt = nullptr;   // points of the open children of every open node
+  int32_t* wnxt_off = nullptr;
   int32_t* tile_sum = nullptr;
   int32_t* tile_off = nullptr;
   int32_t* scal = nullptr;  // device scalars: [0] next open count, [1] error flag
-  // per tile of kTile positions: 1 if the tile holds a position of an open node
-  // this level (the tile kernels return at once for the other tiles)
-  unsigned char* tile_act = nullptr;
 };
 
 // ------------------------------------------------------------------ kernels
@@ -93,96 +97,160 @@ __global__ void k_init_points(const T* __restrict__ in, int64_t n, int d, double
   N1[p] = -1;
 }
 
-__device__ __forceinline__ bool open_node(const NodeMeta* __restrict__ meta, int32_t a, int level,
-                                          int leaf) {
-  if (a < 0) return false;
-  NodeMeta m = meta[a];
-  return m.depth == level && m.count > leaf;
+// Working set of the first level when some roots are already leaves: the points
+// of the open roots, compacted in tree order (wst[t] = -1 for a leaf root).
+template <int D>
+__global__ void k_compact_roots(const double* __restrict__ X, const int32_t* __restrict__ I,
+                                const int32_t* __restrict__ NID, const int32_t* __restrict__ wst,
+                                const int64_t* __restrict__ off, int64_t n,
+                                double* __restrict__ Xo, int32_t* __restrict__ Io,
+                                int32_t* __restrict__ NIDo) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int32_t t = NID[p];
+  const int32_t w0 = wst[t];
+  if (w0 < 0) return;
+  const int64_t w = w0 + (p - off[t]);
+#pragma unroll
+  for (int j = 0; j < D; ++j) Xo[(int64_t)j * n + w] = X[(int64_t)j * n + p];
+  Io[w] = I[p];
+  NIDo[w] = t;
 }
 
-// tile_act[t] = 1 for every tile that a segment of an open node overlaps
-__global__ void k_mark_tiles(const int32_t* __restrict__ act, int m,
-                             const NodeMeta* __restrict__ meta,
-                             unsigned char* __restrict__ tile_act) {
-  const int i = blockIdx.x;
-  if (i >= m) return;
-  const NodeMeta nm = meta[act[i]];
-  const int64_t t0 = nm.start / kTile, t1 = ((int64_t)nm.start + nm.count - 1) / kTile;
-  for (int64_t t = t0 + threadIdx.x; t <= t1; t += blockDim.x) tile_act[t] = 1;
-}
-
-// Segmented min/max over open positions; one atomicMin/atomicMax per segment
-// piece that crosses a warp-chunk boundary, direct atomics for pieces inside.
+// Segmented min/max over the working positions.  Each thread reduces kItems
+// consecutive positions in registers; one segmented warp scan per dimension
+// joins the pieces of runs that cross thread boundaries.  Runs that end
+// inside a warp chunk go straight to atomicMin/atomicMax; the first and last
+// run of every warp chunk are merged per block by thread 0.
 template <int D>
 __global__ void __launch_bounds__(kBT) k_seg_box(const double* __restrict__ X,
                                                  const int32_t* __restrict__ NID,
-                                                 const NodeMeta* __restrict__ meta, int level,
-                                                 int leaf, int64_t n,
-                                                 unsigned long long* __restrict__ keys,
-                                                 const unsigned char* __restrict__ tile_act) {
-  if (tile_act && !tile_act[blockIdx.x]) return;
+                                                 int64_t n, int64_t nw,
+                                                 unsigned long long* __restrict__ keys) {
   constexpr int W = kBT / 32;
-  __shared__ int32_t rec_id[kItems * W][2];
-  __shared__ unsigned long long rec_v[kItems * W][2][2 * D];
+  __shared__ int32_t rec_id[W][2];
+  __shared__ unsigned long long rec_v[W][2][2 * D];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-  for (int it = 0; it < kItems; ++it) {
-    int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    int32_t a = -1;
-    if (p < n) {
-      a = NID[p];
-      if (!open_node(meta, a, level, leaf)) a = -1;
+  const int64_t p0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
+  // node of every position (-1 past the working set), run breaks inside the thread
+  static_assert(kItems == 8, "two int4 / four double2 loads per thread");
+  int32_t a[kItems];
+  // vector loads when the thread's 8 positions are all working positions and
+  // aligned (NID from the pool; X rows start at j * n, even for even n)
+  const bool full = p0 + kItems <= nw;
+  const bool vec = full && (n & 1) == 0 && (reinterpret_cast<uintptr_t>(NID) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  if (vec) {
+    const int4 u = __ldg(reinterpret_cast<const int4*>(NID + p0));
+    const int4 v = __ldg(reinterpret_cast<const int4*>(NID + p0) + 1);
+    a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w, a[4] = v.x, a[5] = v.y, a[6] = v.z, a[7] = v.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) a[i] = p0 + i < nw ? NID[p0 + i] : -1;
+  }
+  unsigned brk = 0;
+#pragma unroll
+  for (int i = 1; i < kItems; ++i) brk |= (a[i] != a[i - 1]) ? (1u << i) : 0u;
+  const int32_t hd = a[0], tl = a[kItems - 1];
+  const bool single = brk == 0;
+  // scan steps that stay inside the tail run (equal ids of open nodes are contiguous)
+  unsigned take = 0;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int32_t au = __shfl_up_sync(0xffffffffu, tl, 1 << s);
+    take |= (lane >= (1 << s) && au == tl) ? (1u << s) : 0u;
+  }
+  const int32_t prev_tl = __shfl_up_sync(0xffffffffu, tl, 1);
+  const int32_t next_hd = __shfl_down_sync(0xffffffffu, hd, 1);
+  const int32_t first_id = __shfl_sync(0xffffffffu, hd, 0);
+  const bool join_prev = lane > 0 && prev_tl == hd;  // head run continues the previous lane's tail
+  const bool tail_end = lane == 31 || next_hd != tl;
+#pragma unroll 1
+  for (int j = 0; j < D; ++j) {
+    // coordinates read as raw 64-bit patterns (NaNs keep their bits)
+    const unsigned long long* __restrict__ Xj =
+        reinterpret_cast<const unsigned long long*>(X) + (int64_t)j * n;
+    unsigned long long kk[kItems];
+    if (vec) {
+#pragma unroll
+      for (int h = 0; h < kItems / 2; ++h) {
+        const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(Xj + p0) + h);
+        kk[2 * h] = dkey_bits(x.x);
+        kk[2 * h + 1] = dkey_bits(x.y);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < kItems; ++i) kk[i] = a[i] >= 0 ? dkey_bits(Xj[p0 + i]) : 0ull;
     }
-    unsigned long long mn[D], mx[D];
+    unsigned long long hmn = kk[0], hmx = kk[0], cmn = kk[0], cmx = kk[0];
+    int32_t ca = a[0];
+    bool head_open = true;
 #pragma unroll
-    for (int j = 0; j < D; ++j) {
-      unsigned long long k = a >= 0 ? dkey(X[(int64_t)j * n + p]) : 0ull;
-      mn[j] = k;
-      mx[j] = k;
-    }
-    // segmented inclusive scan (runs of equal `a` are contiguous)
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int32_t au = __shfl_up_sync(0xffffffffu, a, o);
-      bool take = lane >= o && au == a;
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        unsigned long long u = __shfl_up_sync(0xffffffffu, mn[j], o);
-        unsigned long long v = __shfl_up_sync(0xffffffffu, mx[j], o);
-        if (take) {
-          mn[j] = u < mn[j] ? u : mn[j];
-          mx[j] = v > mx[j] ? v : mx[j];
+    for (int i = 1; i < kItems; ++i) {
+      if (brk & (1u << i)) {
+        if (head_open) {
+          hmn = cmn;
+          hmx = cmx;
+          head_open = false;
+        } else if (ca >= 0) {  // a run that starts and ends inside this thread
+          atomicMin(&keys[(int64_t)ca * 2 * D + 2 * j], cmn);
+          atomicMax(&keys[(int64_t)ca * 2 * D + 2 * j + 1], cmx);
         }
+        ca = a[i];
+        cmn = kk[i];
+        cmx = kk[i];
+      } else {
+        cmn = kk[i] < cmn ? kk[i] : cmn;
+        cmx = kk[i] > cmx ? kk[i] : cmx;
       }
     }
-    int32_t a_next = __shfl_down_sync(0xffffffffu, a, 1);
-    int32_t a0 = __shfl_sync(0xffffffffu, a, 0);
-    bool tail = (lane == 31) || (a_next != a);
-    bool first_run = (a == a0);
-    bool last_run = (a == __shfl_sync(0xffffffffu, a, 31));
-    int chunk = it * W + w;
-    if (tail && a >= 0 && !first_run && !last_run) {
+    // segmented inclusive scan of the tail runs
 #pragma unroll
-      for (int j = 0; j < D; ++j) {
-        atomicMin(&keys[(int64_t)a * 2 * D + 2 * j], mn[j]);
-        atomicMax(&keys[(int64_t)a * 2 * D + 2 * j + 1], mx[j]);
+    for (int s = 0; s < 5; ++s) {
+      const unsigned long long u = __shfl_up_sync(0xffffffffu, cmn, 1 << s);
+      const unsigned long long v = __shfl_up_sync(0xffffffffu, cmx, 1 << s);
+      if (take & (1u << s)) {
+        cmn = u < cmn ? u : cmn;
+        cmx = v > cmx ? v : cmx;
       }
     }
-    if (tail && first_run) {
-      rec_id[chunk][0] = a;
+    const unsigned long long pmn = __shfl_up_sync(0xffffffffu, cmn, 1);
+    const unsigned long long pmx = __shfl_up_sync(0xffffffffu, cmx, 1);
+    // run ends: the head run when it ends inside this thread, the tail run when
+    // the next lane starts another node (or at the end of the chunk)
 #pragma unroll
-      for (int j = 0; j < D; ++j) {
-        rec_v[chunk][0][2 * j] = mn[j];
-        rec_v[chunk][0][2 * j + 1] = mx[j];
+    for (int e = 0; e < 2; ++e) {
+      int32_t id;
+      unsigned long long mn, mx;
+      bool is_end;
+      if (e == 0) {
+        is_end = !single;
+        id = hd;
+        mn = hmn;
+        mx = hmx;
+        if (join_prev) {
+          mn = pmn < mn ? pmn : mn;
+          mx = pmx > mx ? pmx : mx;
+        }
+      } else {
+        is_end = tail_end;
+        id = tl;
+        mn = cmn;
+        mx = cmx;
       }
-    }
-    if (lane == 31) {
-      // the last run; equal to the first run when the whole warp is one run
-      rec_id[chunk][1] = first_run ? -2 : a;
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        rec_v[chunk][1][2 * j] = mn[j];
-        rec_v[chunk][1][2 * j + 1] = mx[j];
+      if (!is_end) continue;
+      if (id == first_id) {
+        if (j == 0) rec_id[w][0] = id;
+        rec_v[w][0][2 * j] = mn;
+        rec_v[w][0][2 * j + 1] = mx;
+        if (lane == 31 && e == 1 && j == 0) rec_id[w][1] = -2;  // one run spans the chunk
+      } else if (e == 1 && lane == 31) {
+        if (j == 0) rec_id[w][1] = id;
+        rec_v[w][1][2 * j] = mn;
+        rec_v[w][1][2 * j + 1] = mx;
+      } else if (id >= 0) {
+        atomicMin(&keys[(int64_t)id * 2 * D + 2 * j], mn);
+        atomicMax(&keys[(int64_t)id * 2 * D + 2 * j + 1], mx);
       }
     }
   }
@@ -199,9 +267,9 @@ __global__ void __launch_bounds__(kBT) k_seg_box(const double* __restrict__ X,
         }
       }
     };
-    for (int c = 0; c < kItems * W; ++c) {
+    for (int c = 0; c < W; ++c) {
       for (int r = 0; r < 2; ++r) {
-        int32_t id = rec_id[c][r];
+        const int32_t id = rec_id[c][r];
         if (id == -2) continue;  // no separate last run
         if (id == cur) {
 #pragma unroll
@@ -279,18 +347,15 @@ __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __res
   ext[a] = 0x7fffffff;
 }
 
-// first position of a sliding segment that holds the extreme value
+// first working position of a sliding segment that holds the extreme value
 __global__ void k_argext(const double* __restrict__ X, const int32_t* __restrict__ NID,
                          const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
-                         int level, int leaf, int64_t n, int32_t* __restrict__ ext,
-                         const unsigned char* __restrict__ tile_act) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  if (!tile_act[p / kTile]) return;
-  int32_t a = NID[p];
-  if (!open_node(meta, a, level, leaf)) return;
+                         int64_t n, int64_t nw, int32_t* __restrict__ ext) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nw) return;
+  const int32_t a = NID[p];
   if (mode[a] == 0) return;
-  NodeMeta m = meta[a];
+  const NodeMeta m = meta[a];
   if (X[(int64_t)m.axis * n + p] == m.split) atomicMin(&ext[a], (int32_t)p);
 }
 
@@ -301,58 +366,91 @@ __device__ __forceinline__ int flag_of(const double* __restrict__ X, int64_t n, 
   return p != ext ? 1 : 0;                                            // :391-403
 }
 
+// Exclusive prefix, in position order, of one tile's 0/1 flags, visited as
+// p = base + it * kBT + threadIdx.x: msk[it] is the warp's ballot of pass it.
+// Leaves in cpre[it * W + w] the offset of warp w's 32 positions of pass it and
+// returns the tile total.  Two barriers per tile.
+__device__ __forceinline__ int32_t tile_chunk_prefix(const unsigned (&msk)[kItems],
+                                                     int32_t* cpre) {
+  constexpr int W = kBT / 32, NC = kItems * W;
+  static_assert(NC == 64, "two warp chunks per lane in the chunk scan");
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) cpre[it * W + w] = __popc(msk[it]);
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int32_t x0 = cpre[2 * lane], x1 = cpre[2 * lane + 1], s = x0 + x1;
+    const int32_t inc = warp_inclusive_scan(s);
+    cpre[2 * lane] = inc - s;
+    cpre[2 * lane + 1] = inc - s + x0;
+    if (lane == 31) cpre[NC] = inc;
+  }
+  __syncthreads();
+  return cpre[NC];
+}
+
 // per-tile left counts and the segment-start / segment-end local prefixes
 __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ NID,
                                                const NodeMeta* __restrict__ meta,
                                                const int32_t* __restrict__ mode,
-                                               const int32_t* __restrict__ ext, int level, int leaf,
-                                               int64_t n, int32_t* __restrict__ tile_sum,
+                                               const int32_t* __restrict__ ext,
+                                               const int32_t* __restrict__ wst, int64_t n,
+                                               int64_t nw, int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
-                                               int32_t* __restrict__ pend,
-                                               const unsigned char* __restrict__ tile_act) {
-  __shared__ int32_t tmp[kBT / 32];
-  if (!tile_act[blockIdx.x]) {
-    if (threadIdx.x == 0) tile_sum[blockIdx.x] = 0;
-    return;
-  }
+                                               int32_t* __restrict__ pend) {
+  constexpr int W = kBT / 32;
+  __shared__ int32_t cpre[kItems * W + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTile;
-  int32_t run = 0;
+  unsigned msk[kItems];
+  int32_t av[kItems];
+  unsigned se = 0;  // bit 2 it: segment start, bit 2 it + 1: segment end
+#pragma unroll
   for (int it = 0; it < kItems; ++it) {
-    int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    int32_t a = p < n ? NID[p] : -1;
+    const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
+    const int32_t a = p < nw ? NID[p] : -1;
     int f = 0;
-    NodeMeta m;
-    if (open_node(meta, a, level, leaf)) {
-      m = meta[a];
-      f = flag_of(X, n, p, m, mode[a], ext[a]);
-    } else {
-      a = -1;
-    }
-    int32_t tot;
-    int32_t ex = block_exclusive_scan<int32_t, kBT>(f, tmp, tot) + run;
     if (a >= 0) {
-      if (p == m.start) pstart[a] = ex;
-      if (p == (int64_t)m.start + m.count - 1) pend[a] = ex + f;
+      const NodeMeta m = meta[a];
+      const int32_t w0 = wst[a];
+      f = flag_of(X, n, p, m, mode[a], ext[a]);
+      if (p == w0) se |= 1u << (2 * it);
+      if (p == (int64_t)w0 + m.count - 1) se |= 2u << (2 * it);
     }
-    run += tot;
+    msk[it] = __ballot_sync(0xffffffffu, f);
+    av[it] = a;
   }
-  if (threadIdx.x == 0) tile_sum[blockIdx.x] = run;
+  const int32_t tot = tile_chunk_prefix(msk, cpre);
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const unsigned b = (se >> (2 * it)) & 3u;
+    if (b == 0) continue;
+    const int32_t ex = cpre[it * W + w] + __popc(msk[it] & lt);
+    if (b & 1u) pstart[av[it]] = ex;
+    if (b & 2u) pend[av[it]] = ex + (int32_t)((msk[it] >> lane) & 1u);
+  }
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
 }
 
-// n_left, child pairs and cells; counts the next open list (cosmokdtree.f90:412-448)
+// n_left, child pairs and cells; counts the next open list and its working
+// points (cosmokdtree.f90:412-448)
 template <int D>
 __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
                            double* __restrict__ cell, const int32_t* __restrict__ pstart,
                            const int32_t* __restrict__ pend, const int32_t* __restrict__ tile_off,
-                           int32_t* __restrict__ nleft, int32_t* __restrict__ pbase,
-                           unsigned long long* __restrict__ keys, int32_t first_child, int leaf,
-                           int32_t* __restrict__ nxt_cnt, int32_t* __restrict__ err) {
+                           const int32_t* __restrict__ wst, int32_t* __restrict__ nleft,
+                           int32_t* __restrict__ pbase, unsigned long long* __restrict__ keys,
+                           int32_t first_child, int leaf, int32_t* __restrict__ nxt_cnt,
+                           int32_t* __restrict__ wcnt, int32_t* __restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int32_t a = act[i];
   NodeMeta pm = meta[a];
-  int64_t s = pm.start, e = (int64_t)pm.start + pm.count - 1;
+  int64_t s = wst[a], e = (int64_t)wst[a] + pm.count - 1;
   int32_t P0 = tile_off[s / kTile] + pstart[a];
   int32_t P1 = tile_off[e / kTile] + pend[a];
   int32_t nl = P1 - P0;
@@ -364,7 +462,7 @@ __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __r
   pbase[a] = P0;
   int32_t c0 = first_child + 2 * i;
   meta[a].left = c0;
-  int cnt = 0;
+  int cnt = 0, pts = 0;
   for (int side = 0; side < 2; ++side) {
     int32_t c = c0 + side;
     NodeMeta cm;
@@ -388,71 +486,95 @@ __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __r
       keys[(int64_t)c * 2 * D + 2 * j] = ~0ull;
       keys[(int64_t)c * 2 * D + 2 * j + 1] = 0ull;
     }
-    if (cm.count > leaf) ++cnt;
+    if (cm.count > leaf) {
+      ++cnt;
+      pts += cm.count;
+    }
   }
   nxt_cnt[i] = cnt;
+  wcnt[i] = pts;
 }
 
-__global__ void k_next_list(const int32_t* __restrict__ act, int m,
-                            const NodeMeta* __restrict__ meta, const int32_t* __restrict__ nxt_off,
-                            int leaf, int32_t* __restrict__ nxt) {
+// next open list (children in list order, so in leaf order) and their working starts
+__global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMeta* __restrict__ meta,
+                            const int32_t* __restrict__ nxt_off,
+                            const int32_t* __restrict__ wnxt_off, int leaf,
+                            int32_t* __restrict__ nxt, int32_t* __restrict__ wst) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  int32_t c0 = meta[act[i]].left;
-  int32_t o = nxt_off[i];
-  if (meta[c0].count > leaf) nxt[o++] = c0;
-  if (meta[c0 + 1].count > leaf) nxt[o] = c0 + 1;
+  const int32_t c0 = meta[act[i]].left;
+  int32_t o = nxt_off[i], w = wnxt_off[i];
+  const int32_t n0 = meta[c0].count, n1 = meta[c0 + 1].count;
+  if (n0 > leaf) {
+    nxt[o++] = c0;
+    wst[c0] = w;
+    w += n0;
+  }
+  if (n1 > leaf) {
+    nxt[o] = c0 + 1;
+    wst[c0 + 1] = w;
+  }
 }
 
-// stable partition of every open segment into the other buffer
+// Stable partition of every open segment: points of open children go to the
+// next working set, points of new leaves to the final leaf-ordered arrays.
 template <int D>
 __global__ void __launch_bounds__(kBT) k_scatter(
     const double* __restrict__ X, const int32_t* __restrict__ I, const int32_t* __restrict__ NID,
     const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
     const int32_t* __restrict__ ext, const int32_t* __restrict__ tile_off,
-    const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase, int level, int leaf,
-    int64_t n, double* __restrict__ Xo, int32_t* __restrict__ Io, int32_t* __restrict__ NIDo,
-    double* __restrict__ Pf, int32_t* __restrict__ If, int32_t* __restrict__ err,
-    const unsigned char* __restrict__ tile_act) {
-  __shared__ int32_t tmp[kBT / 32];
-  if (!tile_act[blockIdx.x]) return;
+    const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase,
+    const int32_t* __restrict__ wst, int leaf, int64_t n, int64_t nw, double* __restrict__ Xo,
+    int32_t* __restrict__ Io, int32_t* __restrict__ NIDo, double* __restrict__ Pf,
+    int32_t* __restrict__ If, int32_t* __restrict__ err) {
+  constexpr int W = kBT / 32;
+  __shared__ int32_t cpre[kItems * W + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTile;
-  int32_t run = tile_off[blockIdx.x];
+  unsigned msk[kItems];
+  int32_t av[kItems];
+#pragma unroll
   for (int it = 0; it < kItems; ++it) {
-    int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    int32_t a = p < n ? NID[p] : -1;
+    const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
+    const int32_t a = p < nw ? NID[p] : -1;
     int f = 0;
-    NodeMeta m;
-    if (open_node(meta, a, level, leaf)) {
-      m = meta[a];
-      f = flag_of(X, n, p, m, mode[a], ext[a]);
-    } else {
-      a = -1;
-    }
-    int32_t tot;
-    int32_t ex = block_exclusive_scan<int32_t, kBT>(f, tmp, tot) + run;
-    run += tot;
+    if (a >= 0) f = flag_of(X, n, p, meta[a], mode[a], ext[a]);
+    msk[it] = __ballot_sync(0xffffffffu, f);
+    av[it] = a;
+  }
+  tile_chunk_prefix(msk, cpre);
+  const int32_t run = tile_off[blockIdx.x];
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const int32_t a = av[it];
     if (a < 0) continue;
-    int32_t rl = ex - pbase[a];
-    int32_t nl = nleft[a];
-    int64_t dst = f ? (int64_t)m.start + rl : (int64_t)m.start + nl + ((p - m.start) - rl);
-    if (dst < m.start || dst >= (int64_t)m.start + m.count) {  // never for a consistent scan
+    const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
+    const int f = (int)((msk[it] >> lane) & 1u);
+    const int32_t ex = run + cpre[it * W + w] + __popc(msk[it] & lt);
+    const NodeMeta m = meta[a];
+    const int32_t rl = ex - pbase[a];  // left points before p in the segment
+    const int32_t nl = nleft[a];
+    const int32_t rank = f ? rl : (int32_t)(p - wst[a]) - rl;  // rank in the child
+    const int32_t ccount = f ? nl : m.count - nl;
+    if (rank < 0 || rank >= ccount) {  // never for a consistent scan
       atomicExch(err, 2);
       continue;
     }
-    int32_t child = m.left + (f ? 0 : 1);
-    int32_t ccount = f ? nl : m.count - nl;
-    int32_t id = I[p];
-    Io[dst] = id;
-    NIDo[dst] = child;
-    bool is_leaf = ccount <= leaf;
+    const int32_t child = m.left + (f ? 0 : 1);
+    const int32_t id = I[p];
+    if (ccount <= leaf) {
+      const int64_t dst = (int64_t)m.start + (f ? 0 : nl) + rank;
 #pragma unroll
-    for (int j = 0; j < D; ++j) {
-      double v = X[(int64_t)j * n + p];
-      Xo[(int64_t)j * n + dst] = v;
-      if (is_leaf) Pf[(int64_t)j * n + dst] = v;
+      for (int j = 0; j < D; ++j) Pf[(int64_t)j * n + dst] = X[(int64_t)j * n + p];
+      If[dst] = id;
+    } else {
+      const int64_t wd = (int64_t)wst[child] + rank;
+#pragma unroll
+      for (int j = 0; j < D; ++j) Xo[(int64_t)j * n + wd] = X[(int64_t)j * n + p];
+      Io[wd] = id;
+      NIDo[wd] = child;
     }
-    if (is_leaf) If[dst] = id;
   }
 }
 
@@ -636,6 +758,7 @@ ckd_status ensure_node_cap(BuildBufs& B, int64_t need, cudaStream_t s) {
   CKD_CUDA(grow(&B.pend, B.cap, nc, s));
   CKD_CUDA(grow(&B.nleft, B.cap, nc, s));
   CKD_CUDA(grow(&B.pbase, B.cap, nc, s));
+  CKD_CUDA(grow(&B.wst, B.cap, nc, s));
   B.cap = nc;
   return CKD_OK;
 }
@@ -643,8 +766,8 @@ ckd_status ensure_node_cap(BuildBufs& B, int64_t need, cudaStream_t s) {
 void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
-                B.nleft,  B.pbase,   B.act[0],    B.act[1],   B.nxt_cnt, B.nxt_off, B.tile_sum,
-                B.tile_off, B.scal, B.tile_act};
+                B.nleft,  B.pbase,   B.wst,       B.act[0],   B.act[1],  B.nxt_cnt, B.nxt_off,
+                B.wcnt,   B.wnxt_off, B.tile_sum, B.tile_off, B.scal};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -673,15 +796,16 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   for (int b = 0; b < 2; ++b) CKD_CUDA(dev_alloc((void**)&B.act[b], sizeof(int32_t) * max_open, s));
   CKD_CUDA(dev_alloc((void**)&B.nxt_cnt, sizeof(int32_t) * max_open, s));
   CKD_CUDA(dev_alloc((void**)&B.nxt_off, sizeof(int32_t) * (max_open + 1), s));
+  CKD_CUDA(dev_alloc((void**)&B.wcnt, sizeof(int32_t) * max_open, s));
+  CKD_CUDA(dev_alloc((void**)&B.wnxt_off, sizeof(int32_t) * (max_open + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.tile_sum, sizeof(int32_t) * ntiles, s));
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
-  CKD_CUDA(dev_alloc((void**)&B.tile_act, (size_t)ntiles, s));
   CKD_CUDA(cudaMemsetAsync(B.scal, 0, sizeof(int32_t) * 4, s));
 
   // final outputs
-  CKD_CUDA(cudaMalloc((void**)&t->pts, sizeof(double) * D * n));
-  CKD_CUDA(cudaMalloc((void**)&t->ids, sizeof(int32_t) * n));
+  CKD_CUDA(dev_alloc((void**)&t->pts, sizeof(double) * D * n, s));
+  CKD_CUDA(dev_alloc((void**)&t->ids, sizeof(int32_t) * n, s));
 
   // trees of a forest: positions off[t] .. off[t+1]-1, root node t
   const int32_t T = (int32_t)t->n_trees;
@@ -709,10 +833,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_LAUNCH_CHECK();
 
   // Root bounding boxes: validation (finite, inside the periodic box) and the
-  // non-periodic root cells.  Computed with the open-node reduction using a leaf
-  // threshold of 0 so that every root is "open" here.
-  k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], B.meta, 0, 0, n, B.keys,
-                                                 nullptr);
+  // non-periodic root cells, from the segmented reduction over every point
+  // (position p belongs to root NID[p]).
+  k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[0], B.NID[0], n, n, B.keys);
   CKD_LAUNCH_CHECK();
   std::vector<unsigned long long> rk((size_t)T * 2 * D);
   CKD_CUDA(cudaMemcpyAsync(rk.data(), B.keys, sizeof(unsigned long long) * 2 * D * T,
@@ -750,22 +873,38 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     k_root_cells<D><<<(unsigned)cdiv(T, 128), 128, 0, s>>>(B.cell, B.keys, T);
     CKD_LAUNCH_CHECK();
   }
-  // points of trees that are a single leaf never move: start from the input order
-  CKD_CUDA(cudaMemcpyAsync(t->pts, B.X[0], sizeof(double) * D * n, cudaMemcpyDeviceToDevice, s));
-  CKD_CUDA(cudaMemcpyAsync(t->ids, B.I[0], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
-  // open roots
+  // open roots and the first working set
   std::vector<int32_t> roots;
+  std::vector<int32_t> wst0((size_t)T, -1);
+  int64_t nw = 0;
   for (int32_t tr = 0; tr < T; ++tr)
-    if (off[tr + 1] - off[tr] > leaf) roots.push_back(tr);
+    if (off[tr + 1] - off[tr] > leaf) {
+      roots.push_back(tr);
+      wst0[tr] = (int32_t)nw;
+      nw += off[tr + 1] - off[tr];
+    }
+  int cur = 0;
+  if (nw < n) {
+    // points of trees that are a single leaf never move: start from the input order
+    CKD_CUDA(cudaMemcpyAsync(t->pts, B.X[0], sizeof(double) * D * n, cudaMemcpyDeviceToDevice, s));
+    CKD_CUDA(cudaMemcpyAsync(t->ids, B.I[0], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+  }
+  CKD_CUDA(cudaMemcpyAsync(B.wst, wst0.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, s));
+  if (nw < n && nw > 0) {
+    k_compact_roots<D><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(B.X[0], B.I[0], B.NID[0], B.wst,
+                                                             off_dev, n, B.X[1], B.I[1], B.NID[1]);
+    CKD_LAUNCH_CHECK();
+    cur = 1;
+  }
   if (!roots.empty())
     CKD_CUDA(cudaMemcpyAsync(B.act[0], roots.data(), sizeof(int32_t) * roots.size(),
                              cudaMemcpyHostToDevice, s));
-  CKD_CUDA(cudaStreamSynchronize(s));  // `roots` and `rk` are host buffers of the copies
+  CKD_CUDA(cudaStreamSynchronize(s));  // `roots`, `wst0` and `rk` are host buffers of the copies
   dev_free(off_dev, s);
 
   int32_t n_nodes = T;
   int m = (int)roots.size();
-  int cur = 0;
+  int alist = 0;  // open list buffer of this level
   int level = 0;
   while (m > 0) {
     if (level >= kMaxLevels) {
@@ -773,43 +912,45 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
       return fail(CKD_ERR_DEPTH, "tree depth exceeds the build's level cap (8192 levels)");
     }
     CKD_TRY(ensure_node_cap(B, (int64_t)n_nodes + 2 * (int64_t)m, s));
-    const int32_t* act = B.act[cur];
-    unsigned gm = (unsigned)cdiv(m, 128);
-    CKD_CUDA(cudaMemsetAsync(B.tile_act, 0, (size_t)ntiles, s));
-    k_mark_tiles<<<(unsigned)m, 128, 0, s>>>(act, m, B.meta, B.tile_act);
-    CKD_LAUNCH_CHECK();
-    if (level > 0) {
-      k_seg_box<D><<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, level, leaf, n,
-                                                    B.keys, B.tile_act);
+    const int32_t* act = B.act[alist];
+    const unsigned gm = (unsigned)cdiv(m, 128);
+    const unsigned ntw = (unsigned)cdiv(nw, kTile);
+    if (level > 0) {  // the roots' boxes come from the validation pass
+      k_seg_box<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], n, nw, B.keys);
       CKD_LAUNCH_CHECK();
     }
     k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
     CKD_LAUNCH_CHECK();
-    k_argext<<<(unsigned)cdiv(n, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, level,
-                                                    leaf, n, B.ext, B.tile_act);
+    k_argext<<<(unsigned)cdiv(nw, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, n, nw,
+                                                     B.ext);
     CKD_LAUNCH_CHECK();
-    k_flags<<<(unsigned)ntiles, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, level,
-                                             leaf, n, B.tile_sum, B.pstart, B.pend, B.tile_act);
+    k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, B.wst, n, nw,
+                                B.tile_sum, B.pstart, B.pend);
     CKD_LAUNCH_CHECK();
-    CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntiles, s));
-    k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off,
-                                     B.nleft, B.pbase, B.keys, n_nodes, leaf, B.nxt_cnt,
+    CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
+    k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off, B.wst,
+                                     B.nleft, B.pbase, B.keys, n_nodes, leaf, B.nxt_cnt, B.wcnt,
                                      B.scal + 1);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.nxt_cnt, B.nxt_off, m, s));
-    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.act[1 - cur]);
+    CKD_TRY(scan_i32(B.wcnt, B.wnxt_off, m, s));
+    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, B.wnxt_off, leaf, B.act[1 - alist],
+                                   B.wst);
     CKD_LAUNCH_CHECK();
-    k_scatter<D><<<(unsigned)ntiles, kBT, 0, s>>>(
-        B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext, B.tile_off, B.nleft, B.pbase,
-        level, leaf, n, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1,
-        B.tile_act);
+    k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext,
+                                     B.tile_off, B.nleft, B.pbase, B.wst, leaf, n, nw,
+                                     B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids,
+                                     B.scal + 1);
     CKD_LAUNCH_CHECK();
-    int32_t nm = 0;
+    int32_t nm = 0, nwn = 0;
     CKD_CUDA(cudaMemcpyAsync(&nm, B.nxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CKD_CUDA(cudaMemcpyAsync(&nwn, B.wnxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
     n_nodes += 2 * m;
     m = nm;
+    nw = nwn;
     cur = 1 - cur;
+    alist = 1 - alist;
     ++level;
   }
   int32_t err = 0;
@@ -821,9 +962,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_LAUNCH_CHECK();
   t->n_nodes = n_nodes;
   t->depth = level;
-  CKD_CUDA(cudaMalloc((void**)&t->meta, sizeof(NodeMeta) * n_nodes));
-  CKD_CUDA(cudaMalloc((void**)&t->box, sizeof(double) * 2 * D * n_nodes));
-  CKD_CUDA(cudaMalloc((void**)&t->cell, sizeof(double) * 2 * D * n_nodes));
+  CKD_CUDA(dev_alloc((void**)&t->meta, sizeof(NodeMeta) * n_nodes, s));
+  CKD_CUDA(dev_alloc((void**)&t->box, sizeof(double) * 2 * D * n_nodes, s));
+  CKD_CUDA(dev_alloc((void**)&t->cell, sizeof(double) * 2 * D * n_nodes, s));
   CKD_CUDA(cudaMemcpyAsync(t->meta, B.meta, sizeof(NodeMeta) * n_nodes, cudaMemcpyDeviceToDevice, s));
   CKD_CUDA(cudaMemcpyAsync(t->box, B.box, sizeof(double) * 2 * D * n_nodes, cudaMemcpyDeviceToDevice, s));
   CKD_CUDA(cudaMemcpyAsync(t->cell, B.cell, sizeof(double) * 2 * D * n_nodes, cudaMemcpyDeviceToDevice, s));
@@ -837,9 +978,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     t->slack[j] = (float)(b * (1.0 + 1e-6));
   }
   constexpr int NV = (D + 3) / 4;
-  CKD_CUDA(cudaMalloc((void**)&t->box32, sizeof(float) * 2 * D * n_nodes));
-  CKD_CUDA(cudaMalloc((void**)&t->pts32, sizeof(float4) * NV * n));
-  CKD_CUDA(cudaMalloc((void**)&t->pts64, sizeof(double4) * NV * n));
+  CKD_CUDA(dev_alloc((void**)&t->box32, sizeof(float) * 2 * D * n_nodes, s));
+  CKD_CUDA(dev_alloc((void**)&t->pts32, sizeof(float4) * NV * n, s));
+  CKD_CUDA(dev_alloc((void**)&t->pts64, sizeof(double4) * NV * n, s));
   k_pts64<D><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(t->pts, n, t->pts64);
   CKD_LAUNCH_CHECK();
   k_box32<D><<<(unsigned)cdiv((int64_t)n_nodes * 2 * D, 256), 256, 0, s>>>(t->box, n_nodes, t->box32);
@@ -847,9 +988,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   k_pts32<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(t->meta, n_nodes, leaf, t->box, t->pts, n,
                                                           t->pts32);
   CKD_LAUNCH_CHECK();
-  CKD_CUDA(cudaMalloc((void**)&t->pair, sizeof(float4) * pair_f4(D) * n_nodes));
-  CKD_CUDA(cudaMalloc((void**)&t->cell32, sizeof(float) * 2 * D * n_nodes));
-  CKD_CUDA(cudaMalloc((void**)&t->centre, sizeof(double) * D * n_nodes));
+  CKD_CUDA(dev_alloc((void**)&t->pair, sizeof(float4) * pair_f4(D) * n_nodes, s));
+  CKD_CUDA(dev_alloc((void**)&t->cell32, sizeof(float) * 2 * D * n_nodes, s));
+  CKD_CUDA(dev_alloc((void**)&t->centre, sizeof(double) * D * n_nodes, s));
   k_search_records<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(
       t->meta, n_nodes, t->box, t->cell, t->pair, t->cell32, t->centre);
   CKD_LAUNCH_CHECK();

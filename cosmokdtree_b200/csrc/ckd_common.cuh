@@ -146,9 +146,11 @@ __device__ __forceinline__ double axis_gap(double x, double lo, double hi, doubl
 // ------------------------------------------------------ ordered double keys
 // Monotone map double -> uint64 so that atomicMin/atomicMax on the key order
 // doubles (NaNs sort beyond the infinities).
-__device__ __forceinline__ unsigned long long dkey(double x) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(x);
+__device__ __forceinline__ unsigned long long dkey_bits(unsigned long long b) {
   return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  return dkey_bits((unsigned long long)__double_as_longlong(x));
 }
 __device__ __forceinline__ double dkey_inv(unsigned long long k) {
   unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;

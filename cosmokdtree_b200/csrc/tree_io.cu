@@ -145,7 +145,7 @@ ckd_status ckd_tree_load(const char* path, ckd_tree** out) {
       st = fail(CKD_ERR_BAD_ARG, std::string(path) + ": truncated");
       break;
     }
-    cudaError_t e = cudaMalloc(a.dev, a.bytes);
+    cudaError_t e = dev_alloc(a.dev, a.bytes, 0);  // legacy stream: ordered before the copy
     if (e == cudaSuccess) e = cudaMemcpy(*a.dev, buf.data(), a.bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) st = cuda_fail(e, "uploading a saved tree");
   }

@@ -34,7 +34,7 @@ from ._lib import CKDArgumentError, check
 __all__ = [
     "KDTree", "build_kdtree", "deallocate_kdtree", "knn_search", "ball_search", "box_search",
     "knn_search_batch", "ball_search_csr", "box_search_csr", "box_search_periodic_csr",
-    "save_kdtree", "load_kdtree", "read_fortran_points",
+    "save_kdtree", "load_kdtree", "read_fortran_points", "release_cached_memory",
 ]
 
 
@@ -189,8 +189,17 @@ def build_kdtree(points, leaf=None, boxsize=None) -> KDTree:
 
 
 def deallocate_kdtree(tree: KDTree) -> None:
-    """Free the tree's device memory (kdtree.py:37-38)."""
+    """Free the tree's device memory (kdtree.py:37-38).  The memory returns to the
+    library's device pool, where the next build reuses it."""
     tree.close()
+
+
+def release_cached_memory(device: int | None = None) -> None:
+    """Hand the memory cached in the library's pool on ``device`` (freed trees and
+    build scratch) back to the driver, e.g. before a large PyTorch allocation."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    with torch.cuda.device(dev):
+        check(_lib.load().ckd_release_cached_memory())
 
 
 # ---------------------------------------------------------------- kNN

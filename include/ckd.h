@@ -59,8 +59,14 @@ ckd_status ckd_build(const void* pts, int64_t n, int d, int dtype, int leaf,
                      const double* boxsize, int pts_on_device, void* stream, ckd_tree** out);
 
 /* Free a tree and its device buffers (replaces pydeallocate_tree,
- * src/cosmokdtree2py.f90:80-97).  NULL is accepted. */
+ * src/cosmokdtree2py.f90:80-97).  NULL is accepted.  Waits for the device to
+ * finish pending work; the memory returns to the library's device pool, where
+ * the next build reuses it. */
 ckd_status ckd_free(ckd_tree* tree);
+
+/* Return the memory cached in the current device's pool (freed trees and
+ * scratch) to the driver.  No reference counterpart. */
+ckd_status ckd_release_cached_memory(void);
 
 /* Scalar properties of a built tree.  Any output pointer may be NULL. */
 ckd_status ckd_tree_info(const ckd_tree* tree, int64_t* n, int* d, int* leaf, int* periodic,

@@ -296,3 +296,28 @@ def test_gpu_periodic_box_wraps(gpu):
     np.testing.assert_array_equal(i2, np.sort(kd.box_search(t, inner[0])))
     with pytest.raises(AssertionError):
         kd.box_search_periodic_csr(kd.build_kdtree(P), inner)
+
+
+@pytest.mark.gpu
+def test_gpu_pool_reuse_and_release(gpu):
+    """Freed trees return to the library pool; rebuilding from reused memory and
+    after handing the cache back to the driver gives identical trees."""
+    import torch
+    kd = gpu.kdtree
+    P = np.random.default_rng(5).random((300_000, 3)) - 0.5
+    ref = kd.build_kdtree(P, boxsize=[1.0, 1.0, 1.0]).export()
+    for _ in range(2):
+        t = kd.build_kdtree(P, boxsize=[1.0, 1.0, 1.0])
+        e = t.export()
+        kd.deallocate_kdtree(t)
+        for key in ref:
+            np.testing.assert_array_equal(e[key], ref[key])
+    free0 = torch.cuda.mem_get_info()[0]
+    kd.release_cached_memory()
+    assert torch.cuda.mem_get_info()[0] >= free0
+    t = kd.build_kdtree(P, boxsize=[1.0, 1.0, 1.0])
+    e = t.export()
+    for key in ref:
+        np.testing.assert_array_equal(e[key], ref[key])
+    d, i = kd.knn_search(t, P[:5], 3)
+    assert (i[:, 0] == np.arange(5)).all()
