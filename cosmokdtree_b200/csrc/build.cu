@@ -5,8 +5,9 @@
 //
 //   k_seg_box     per-node bounding box of the open nodes (segmented min/max)
 //   k_decide      axis (longest cell side, spread tie-break), midpoint, slide mode
-//   k_argext      slide point = first position holding the extreme (atomicMin)
-//   k_flags       left/right flag per position, per-tile sums, segment-end prefixes
+//   k_flags       left flag per position of a midpoint split, per-tile sums and
+//                 segment-end prefixes; slide point of a sliding split = first
+//                 position holding the extreme (atomicMin)
 //   scan          tile offsets
 //   k_children    n_left per node, child pairs, child cells, next open list
 //   k_scatter     stable out-of-place partition into the other buffer; points of
@@ -60,10 +61,10 @@ struct BuildBufs {
   int32_t* wst = nullptr;              // first working position of an open node
   // per level
   int32_t* act[2] = {nullptr, nullptr};
-  int32_t* nxt_cnt = nullptr;
-  int32_t* nxt_off = nullptr;
-  int32_t* wcnt = nullptr;   // points of the open children of every open node
-  int32_t* wnxt_off = nullptr;
+  // per open node: (open children << 32) | points of the open children, and
+  // the exclusive prefix of that (next list slot, next working start)
+  int64_t* nxt_cnt = nullptr;
+  int64_t* nxt_off = nullptr;
   int32_t* tile_sum = nullptr;
   int32_t* tile_off = nullptr;
   int32_t* scal = nullptr;  // device scalars: [0] next open count, [1] error flag
@@ -347,25 +348,6 @@ __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __res
   ext[a] = 0x7fffffff;
 }
 
-// first working position of a sliding segment that holds the extreme value
-__global__ void k_argext(const double* __restrict__ X, const int32_t* __restrict__ NID,
-                         const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
-                         int64_t n, int64_t nw, int32_t* __restrict__ ext) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nw) return;
-  const int32_t a = NID[p];
-  if (mode[a] == 0) return;
-  const NodeMeta m = meta[a];
-  if (X[(int64_t)m.axis * n + p] == m.split) atomicMin(&ext[a], (int32_t)p);
-}
-
-__device__ __forceinline__ int flag_of(const double* __restrict__ X, int64_t n, int64_t p,
-                                       const NodeMeta& m, int md, int32_t ext) {
-  if (md == 0) return X[(int64_t)m.axis * n + p] < m.split ? 1 : 0;  // :470
-  if (md == 1) return p == ext ? 1 : 0;                               // :376-388
-  return p != ext ? 1 : 0;                                            // :391-403
-}
-
 // Exclusive prefix, in position order, of one tile's 0/1 flags, visited as
 // p = base + it * kBT + threadIdx.x: msk[it] is the warp's ballot of pass it.
 // Leaves in cpre[it * W + w] the offset of warp w's 32 positions of pass it and
@@ -391,12 +373,15 @@ __device__ __forceinline__ int32_t tile_chunk_prefix(const unsigned (&msk)[kItem
   return cpre[NC];
 }
 
-// per-tile left counts and the segment-start / segment-end local prefixes
+// Per-tile left counts and the segment-start / segment-end local prefixes of the
+// midpoint splits (x < split goes left, cosmokdtree.f90:470).  A sliding split
+// sends exactly one point, the first holding the extreme (:376-403), to the
+// side that would be empty; its positions count 0 here and record that point.
 __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ NID,
                                                const NodeMeta* __restrict__ meta,
                                                const int32_t* __restrict__ mode,
-                                               const int32_t* __restrict__ ext,
+                                               int32_t* __restrict__ ext,
                                                const int32_t* __restrict__ wst, int64_t n,
                                                int64_t nw, int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
@@ -416,7 +401,9 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
     if (a >= 0) {
       const NodeMeta m = meta[a];
       const int32_t w0 = wst[a];
-      f = flag_of(X, n, p, m, mode[a], ext[a]);
+      const double x = X[(int64_t)m.axis * n + p];
+      if (mode[a] == 0) f = x < m.split ? 1 : 0;
+      else if (x == m.split) atomicMin(&ext[a], (int32_t)p);
       if (p == w0) se |= 1u << (2 * it);
       if (p == (int64_t)w0 + m.count - 1) se |= 2u << (2 * it);
     }
@@ -442,18 +429,26 @@ template <int D>
 __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
                            double* __restrict__ cell, const int32_t* __restrict__ pstart,
                            const int32_t* __restrict__ pend, const int32_t* __restrict__ tile_off,
-                           const int32_t* __restrict__ wst, int32_t* __restrict__ nleft,
+                           const int32_t* __restrict__ wst, const int32_t* __restrict__ mode,
+                           const int32_t* __restrict__ ext, int32_t* __restrict__ nleft,
                            int32_t* __restrict__ pbase, unsigned long long* __restrict__ keys,
-                           int32_t first_child, int leaf, int32_t* __restrict__ nxt_cnt,
-                           int32_t* __restrict__ wcnt, int32_t* __restrict__ err) {
+                           int32_t first_child, int leaf, int64_t* __restrict__ nxt_cnt,
+                           int32_t* __restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int32_t a = act[i];
   NodeMeta pm = meta[a];
-  int64_t s = wst[a], e = (int64_t)wst[a] + pm.count - 1;
-  int32_t P0 = tile_off[s / kTile] + pstart[a];
-  int32_t P1 = tile_off[e / kTile] + pend[a];
-  int32_t nl = P1 - P0;
+  const int md = mode[a];
+  int32_t nl, P0 = 0;
+  if (md == 0) {
+    int64_t s = wst[a], e = (int64_t)wst[a] + pm.count - 1;
+    P0 = tile_off[s / kTile] + pstart[a];
+    int32_t P1 = tile_off[e / kTile] + pend[a];
+    nl = P1 - P0;
+  } else {
+    nl = md == 1 ? 1 : pm.count - 1;
+    if (ext[a] == 0x7fffffff) nl = 0;  // no slide point found: flagged below
+  }
   if (nl <= 0 || nl >= pm.count) {  // cannot happen for a valid sliding-midpoint split
     atomicExch(err, 1);
     nl = nl <= 0 ? 1 : pm.count - 1;
@@ -491,19 +486,17 @@ __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __r
       pts += cm.count;
     }
   }
-  nxt_cnt[i] = cnt;
-  wcnt[i] = pts;
+  nxt_cnt[i] = ((int64_t)cnt << 32) | (int64_t)pts;
 }
 
 // next open list (children in list order, so in leaf order) and their working starts
 __global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMeta* __restrict__ meta,
-                            const int32_t* __restrict__ nxt_off,
-                            const int32_t* __restrict__ wnxt_off, int leaf,
+                            const int64_t* __restrict__ nxt_off, int leaf,
                             int32_t* __restrict__ nxt, int32_t* __restrict__ wst) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const int32_t c0 = meta[act[i]].left;
-  int32_t o = nxt_off[i], w = wnxt_off[i];
+  int32_t o = (int32_t)(nxt_off[i] >> 32), w = (int32_t)(nxt_off[i] & 0xffffffffll);
   const int32_t n0 = meta[c0].count, n1 = meta[c0 + 1].count;
   if (n0 > leaf) {
     nxt[o++] = c0;
@@ -538,7 +531,10 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
     const int32_t a = p < nw ? NID[p] : -1;
     int f = 0;
-    if (a >= 0) f = flag_of(X, n, p, meta[a], mode[a], ext[a]);
+    if (a >= 0 && mode[a] == 0) {
+      const NodeMeta m = meta[a];
+      f = X[(int64_t)m.axis * n + p] < m.split ? 1 : 0;
+    }
     msk[it] = __ballot_sync(0xffffffffu, f);
     av[it] = a;
   }
@@ -550,12 +546,23 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     const int32_t a = av[it];
     if (a < 0) continue;
     const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    const int f = (int)((msk[it] >> lane) & 1u);
-    const int32_t ex = run + cpre[it * W + w] + __popc(msk[it] & lt);
     const NodeMeta m = meta[a];
-    const int32_t rl = ex - pbase[a];  // left points before p in the segment
+    const int md = mode[a];
     const int32_t nl = nleft[a];
-    const int32_t rank = f ? rl : (int32_t)(p - wst[a]) - rl;  // rank in the child
+    const int32_t q = (int32_t)(p - wst[a]);  // position in the segment
+    int f;
+    int32_t rank;  // rank in the child
+    if (md == 0) {
+      f = (int)((msk[it] >> lane) & 1u);
+      const int32_t ex = run + cpre[it * W + w] + __popc(msk[it] & lt);
+      const int32_t rl = ex - pbase[a];  // left points before p in the segment
+      rank = f ? rl : q - rl;
+    } else {  // the slide point alone on one side, the others keep their order
+      const int32_t e = ext[a];
+      const bool sp = p == e;
+      f = (md == 1) == sp ? 1 : 0;
+      rank = sp ? 0 : q - (p > e ? 1 : 0);
+    }
     const int32_t ccount = f ? nl : m.count - nl;
     if (rank < 0 || rank >= ccount) {  // never for a consistent scan
       atomicExch(err, 2);
@@ -767,7 +774,7 @@ void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
                 B.nleft,  B.pbase,   B.wst,       B.act[0],   B.act[1],  B.nxt_cnt, B.nxt_off,
-                B.wcnt,   B.wnxt_off, B.tile_sum, B.tile_off, B.scal};
+                B.tile_sum, B.tile_off, B.scal};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -794,10 +801,8 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   }
   int64_t max_open = n / (leaf + 1) + 2 + t->n_trees;
   for (int b = 0; b < 2; ++b) CKD_CUDA(dev_alloc((void**)&B.act[b], sizeof(int32_t) * max_open, s));
-  CKD_CUDA(dev_alloc((void**)&B.nxt_cnt, sizeof(int32_t) * max_open, s));
-  CKD_CUDA(dev_alloc((void**)&B.nxt_off, sizeof(int32_t) * (max_open + 1), s));
-  CKD_CUDA(dev_alloc((void**)&B.wcnt, sizeof(int32_t) * max_open, s));
-  CKD_CUDA(dev_alloc((void**)&B.wnxt_off, sizeof(int32_t) * (max_open + 1), s));
+  CKD_CUDA(dev_alloc((void**)&B.nxt_cnt, sizeof(int64_t) * max_open, s));
+  CKD_CUDA(dev_alloc((void**)&B.nxt_off, sizeof(int64_t) * (max_open + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.tile_sum, sizeof(int32_t) * ntiles, s));
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
@@ -921,34 +926,28 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     }
     k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
     CKD_LAUNCH_CHECK();
-    k_argext<<<(unsigned)cdiv(nw, 256), 256, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, n, nw,
-                                                     B.ext);
-    CKD_LAUNCH_CHECK();
     k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, B.wst, n, nw,
                                 B.tile_sum, B.pstart, B.pend);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
     k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off, B.wst,
-                                     B.nleft, B.pbase, B.keys, n_nodes, leaf, B.nxt_cnt, B.wcnt,
-                                     B.scal + 1);
+                                     B.mode, B.ext, B.nleft, B.pbase, B.keys, n_nodes, leaf,
+                                     B.nxt_cnt, B.scal + 1);
     CKD_LAUNCH_CHECK();
-    CKD_TRY(scan_i32(B.nxt_cnt, B.nxt_off, m, s));
-    CKD_TRY(scan_i32(B.wcnt, B.wnxt_off, m, s));
-    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, B.wnxt_off, leaf, B.act[1 - alist],
-                                   B.wst);
+    CKD_TRY(scan_i64(B.nxt_cnt, B.nxt_off, m, s));
+    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.act[1 - alist], B.wst);
     CKD_LAUNCH_CHECK();
     k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext,
                                      B.tile_off, B.nleft, B.pbase, B.wst, leaf, n, nw,
                                      B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids,
                                      B.scal + 1);
     CKD_LAUNCH_CHECK();
-    int32_t nm = 0, nwn = 0;
-    CKD_CUDA(cudaMemcpyAsync(&nm, B.nxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    CKD_CUDA(cudaMemcpyAsync(&nwn, B.wnxt_off + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    int64_t tot = 0;
+    CKD_CUDA(cudaMemcpyAsync(&tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
     n_nodes += 2 * m;
-    m = nm;
-    nw = nwn;
+    m = (int)(tot >> 32);
+    nw = tot & 0xffffffffll;
     cur = 1 - cur;
     alist = 1 - alist;
     ++level;
