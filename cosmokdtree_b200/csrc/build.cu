@@ -67,6 +67,7 @@ struct BuildBufs {
   int64_t* nxt_off = nullptr;
   int32_t* tile_sum = nullptr;
   int32_t* tile_off = nullptr;
+  unsigned* flags = nullptr;  // left flags of the working positions, one bit each
   int32_t* scal = nullptr;  // device scalars: [0] next open count, [1] error flag
 };
 
@@ -385,7 +386,8 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ wst, int64_t n,
                                                int64_t nw, int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
-                                               int32_t* __restrict__ pend) {
+                                               int32_t* __restrict__ pend,
+                                               unsigned* __restrict__ flags) {
   constexpr int W = kBT / 32;
   __shared__ int32_t cpre[kItems * W + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -409,6 +411,7 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
     }
     msk[it] = __ballot_sync(0xffffffffu, f);
     av[it] = a;
+    if (lane == 0) flags[(base >> 5) + it * W + w] = msk[it];
   }
   const int32_t tot = tile_chunk_prefix(msk, cpre);
   const unsigned lt = (1u << lane) - 1u;
@@ -517,9 +520,9 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
     const int32_t* __restrict__ ext, const int32_t* __restrict__ tile_off,
     const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase,
-    const int32_t* __restrict__ wst, int leaf, int64_t n, int64_t nw, double* __restrict__ Xo,
-    int32_t* __restrict__ Io, int32_t* __restrict__ NIDo, double* __restrict__ Pf,
-    int32_t* __restrict__ If, int32_t* __restrict__ err) {
+    const int32_t* __restrict__ wst, const unsigned* __restrict__ flags, int leaf, int64_t n,
+    int64_t nw, double* __restrict__ Xo, int32_t* __restrict__ Io, int32_t* __restrict__ NIDo,
+    double* __restrict__ Pf, int32_t* __restrict__ If, int32_t* __restrict__ err) {
   constexpr int W = kBT / 32;
   __shared__ int32_t cpre[kItems * W + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -529,14 +532,8 @@ __global__ void __launch_bounds__(kBT) k_scatter(
 #pragma unroll
   for (int it = 0; it < kItems; ++it) {
     const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    const int32_t a = p < nw ? NID[p] : -1;
-    int f = 0;
-    if (a >= 0 && mode[a] == 0) {
-      const NodeMeta m = meta[a];
-      f = X[(int64_t)m.axis * n + p] < m.split ? 1 : 0;
-    }
-    msk[it] = __ballot_sync(0xffffffffu, f);
-    av[it] = a;
+    av[it] = p < nw ? NID[p] : -1;
+    msk[it] = flags[(base >> 5) + it * W + w];  // the flag pass's ballot of these 32 positions
   }
   tile_chunk_prefix(msk, cpre);
   const int32_t run = tile_off[blockIdx.x];
@@ -774,7 +771,7 @@ void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
                 B.nleft,  B.pbase,   B.wst,       B.act[0],   B.act[1],  B.nxt_cnt, B.nxt_off,
-                B.tile_sum, B.tile_off, B.scal};
+                B.tile_sum, B.tile_off, B.scal, B.flags};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -805,6 +802,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(dev_alloc((void**)&B.nxt_off, sizeof(int64_t) * (max_open + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.tile_sum, sizeof(int32_t) * ntiles, s));
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
+  CKD_CUDA(dev_alloc((void**)&B.flags, sizeof(unsigned) * ntiles * (kTile / 32), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
   CKD_CUDA(cudaMemsetAsync(B.scal, 0, sizeof(int32_t) * 4, s));
 
@@ -907,6 +905,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(cudaStreamSynchronize(s));  // `roots`, `wst0` and `rk` are host buffers of the copies
   dev_free(off_dev, s);
 
+  // pinned word for the per-level readback of (next open count, next working size)
+  static thread_local int64_t* level_tot = nullptr;
+  if (!level_tot) CKD_CUDA(cudaMallocHost((void**)&level_tot, sizeof(int64_t)));
   int32_t n_nodes = T;
   int m = (int)roots.size();
   int alist = 0;  // open list buffer of this level
@@ -927,7 +928,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
     CKD_LAUNCH_CHECK();
     k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, B.wst, n, nw,
-                                B.tile_sum, B.pstart, B.pend);
+                                B.tile_sum, B.pstart, B.pend, B.flags);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
     k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off, B.wst,
@@ -938,13 +939,13 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.act[1 - alist], B.wst);
     CKD_LAUNCH_CHECK();
     k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext,
-                                     B.tile_off, B.nleft, B.pbase, B.wst, leaf, n, nw,
+                                     B.tile_off, B.nleft, B.pbase, B.wst, B.flags, leaf, n, nw,
                                      B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids,
                                      B.scal + 1);
     CKD_LAUNCH_CHECK();
-    int64_t tot = 0;
-    CKD_CUDA(cudaMemcpyAsync(&tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CKD_CUDA(cudaMemcpyAsync(level_tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
+    const int64_t tot = *level_tot;
     n_nodes += 2 * m;
     m = (int)(tot >> 32);
     nw = tot & 0xffffffffll;
