@@ -40,6 +40,16 @@ constexpr int kItems = 8;         // passes per tile
 constexpr int kTile = kBT * kItems;
 constexpr int kMaxLevels = 8192;  // depth guard (degenerate duplicate clusters peel one point per level)
 
+// What the flag pass needs of an open node, in one 32-byte record.
+struct __align__(16) FlagRec {
+  double split;
+  int32_t axis, md, wst, count;
+  int32_t pad[2];
+};
+
+// What the scatter needs of an open node, in two int4: {start, wst, nleft, count}
+// and {pbase (midpoint split) or slide point, left child, working start of the
+// left / right child or -1 for a leaf child, -2 for the slide point's leaf}.
 struct BuildBufs {
   int d = 0;
   int64_t n = 0;
@@ -59,6 +69,8 @@ struct BuildBufs {
   int32_t* nleft = nullptr;
   int32_t* pbase = nullptr;
   int32_t* wst = nullptr;              // first working position of an open node
+  FlagRec* frec = nullptr;
+  int4* srec = nullptr;                // [cap][2]
   // per level
   int32_t* act[2] = {nullptr, nullptr};
   // per open node: (open children << 32) | points of the open children, and
@@ -296,7 +308,8 @@ template <int D>
 __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
                          double* __restrict__ cell, double* __restrict__ box,
                          const unsigned long long* __restrict__ keys, int32_t* __restrict__ mode,
-                         int32_t* __restrict__ ext) {
+                         int32_t* __restrict__ ext, const int32_t* __restrict__ wst,
+                         FlagRec* __restrict__ frec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int32_t a = act[i];
@@ -347,6 +360,14 @@ __global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __res
   meta[a].axis = axis;
   mode[a] = md;
   ext[a] = 0x7fffffff;
+  FlagRec r;
+  r.split = mid;
+  r.axis = axis;
+  r.md = md;
+  r.wst = wst[a];
+  r.count = meta[a].count;
+  r.pad[0] = r.pad[1] = 0;
+  frec[a] = r;
 }
 
 // Exclusive prefix, in position order, of one tile's 0/1 flags, visited as
@@ -380,10 +401,8 @@ __device__ __forceinline__ int32_t tile_chunk_prefix(const unsigned (&msk)[kItem
 // side that would be empty; its positions count 0 here and record that point.
 __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ NID,
-                                               const NodeMeta* __restrict__ meta,
-                                               const int32_t* __restrict__ mode,
-                                               int32_t* __restrict__ ext,
-                                               const int32_t* __restrict__ wst, int64_t n,
+                                               const FlagRec* __restrict__ frec,
+                                               int32_t* __restrict__ ext, int64_t n,
                                                int64_t nw, int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
                                                int32_t* __restrict__ pend,
@@ -401,13 +420,12 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
     const int32_t a = p < nw ? NID[p] : -1;
     int f = 0;
     if (a >= 0) {
-      const NodeMeta m = meta[a];
-      const int32_t w0 = wst[a];
-      const double x = X[(int64_t)m.axis * n + p];
-      if (mode[a] == 0) f = x < m.split ? 1 : 0;
-      else if (x == m.split) atomicMin(&ext[a], (int32_t)p);
-      if (p == w0) se |= 1u << (2 * it);
-      if (p == (int64_t)w0 + m.count - 1) se |= 2u << (2 * it);
+      const FlagRec r = frec[a];
+      const double x = X[(int64_t)r.axis * n + p];
+      if (r.md == 0) f = x < r.split ? 1 : 0;
+      else if (x == r.split) atomicMin(&ext[a], (int32_t)p);
+      if (p == r.wst) se |= 1u << (2 * it);
+      if (p == (int64_t)r.wst + r.count - 1) se |= 2u << (2 * it);
     }
     msk[it] = __ballot_sync(0xffffffffu, f);
     av[it] = a;
@@ -495,21 +513,32 @@ __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __r
 // next open list (children in list order, so in leaf order) and their working starts
 __global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMeta* __restrict__ meta,
                             const int64_t* __restrict__ nxt_off, int leaf,
-                            int32_t* __restrict__ nxt, int32_t* __restrict__ wst) {
+                            const int32_t* __restrict__ mode, const int32_t* __restrict__ ext,
+                            const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase,
+                            int32_t* __restrict__ nxt, int32_t* __restrict__ wst,
+                            int4* __restrict__ srec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const int32_t c0 = meta[act[i]].left;
+  const int32_t a = act[i];
+  const NodeMeta pm = meta[a];
+  const int32_t c0 = pm.left;
   int32_t o = (int32_t)(nxt_off[i] >> 32), w = (int32_t)(nxt_off[i] & 0xffffffffll);
   const int32_t n0 = meta[c0].count, n1 = meta[c0 + 1].count;
+  const int md = mode[a];
+  int32_t wl = md == 1 ? -2 : -1, wr = md == 2 ? -2 : -1;
   if (n0 > leaf) {
     nxt[o++] = c0;
     wst[c0] = w;
+    wl = w;
     w += n0;
   }
   if (n1 > leaf) {
     nxt[o] = c0 + 1;
     wst[c0 + 1] = w;
+    wr = w;
   }
+  srec[2 * (int64_t)a] = make_int4(pm.start, wst[a], nleft[a], pm.count);
+  srec[2 * (int64_t)a + 1] = make_int4(md == 0 ? pbase[a] : ext[a], c0, wl, wr);
 }
 
 // Stable partition of every open segment: points of open children go to the
@@ -517,12 +546,10 @@ __global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMe
 template <int D>
 __global__ void __launch_bounds__(kBT) k_scatter(
     const double* __restrict__ X, const int32_t* __restrict__ I, const int32_t* __restrict__ NID,
-    const NodeMeta* __restrict__ meta, const int32_t* __restrict__ mode,
-    const int32_t* __restrict__ ext, const int32_t* __restrict__ tile_off,
-    const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase,
-    const int32_t* __restrict__ wst, const unsigned* __restrict__ flags, int leaf, int64_t n,
-    int64_t nw, double* __restrict__ Xo, int32_t* __restrict__ Io, int32_t* __restrict__ NIDo,
-    double* __restrict__ Pf, int32_t* __restrict__ If, int32_t* __restrict__ err) {
+    const int4* __restrict__ srec, const int32_t* __restrict__ tile_off,
+    const unsigned* __restrict__ flags, int64_t n, int64_t nw, double* __restrict__ Xo,
+    int32_t* __restrict__ Io, int32_t* __restrict__ NIDo, double* __restrict__ Pf,
+    int32_t* __restrict__ If, int32_t* __restrict__ err) {
   constexpr int W = kBT / 32;
   __shared__ int32_t cpre[kItems * W + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -543,41 +570,39 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     const int32_t a = av[it];
     if (a < 0) continue;
     const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    const NodeMeta m = meta[a];
-    const int md = mode[a];
-    const int32_t nl = nleft[a];
-    const int32_t q = (int32_t)(p - wst[a]);  // position in the segment
+    const int4 r0 = srec[2 * (int64_t)a], r1 = srec[2 * (int64_t)a + 1];
+    const int32_t start = r0.x, nl = r0.z, count = r0.w;
+    const int32_t q = (int32_t)(p - r0.y);  // position in the segment
     int f;
     int32_t rank;  // rank in the child
-    if (md == 0) {
+    if (r1.z == -2 || r1.w == -2) {  // the slide point alone on one side, the others keep their order
+      const bool sp = p == r1.x;
+      f = (r1.z == -2) == sp ? 1 : 0;
+      rank = sp ? 0 : q - (p > r1.x ? 1 : 0);
+    } else {
       f = (int)((msk[it] >> lane) & 1u);
       const int32_t ex = run + cpre[it * W + w] + __popc(msk[it] & lt);
-      const int32_t rl = ex - pbase[a];  // left points before p in the segment
+      const int32_t rl = ex - r1.x;  // left points before p in the segment
       rank = f ? rl : q - rl;
-    } else {  // the slide point alone on one side, the others keep their order
-      const int32_t e = ext[a];
-      const bool sp = p == e;
-      f = (md == 1) == sp ? 1 : 0;
-      rank = sp ? 0 : q - (p > e ? 1 : 0);
     }
-    const int32_t ccount = f ? nl : m.count - nl;
+    const int32_t ccount = f ? nl : count - nl;
     if (rank < 0 || rank >= ccount) {  // never for a consistent scan
       atomicExch(err, 2);
       continue;
     }
-    const int32_t child = m.left + (f ? 0 : 1);
     const int32_t id = I[p];
-    if (ccount <= leaf) {
-      const int64_t dst = (int64_t)m.start + (f ? 0 : nl) + rank;
+    const int32_t wc = f ? r1.z : r1.w;  // child's working start, negative for a leaf
+    if (wc < 0) {
+      const int64_t dst = (int64_t)start + (f ? 0 : nl) + rank;
 #pragma unroll
       for (int j = 0; j < D; ++j) Pf[(int64_t)j * n + dst] = X[(int64_t)j * n + p];
       If[dst] = id;
     } else {
-      const int64_t wd = (int64_t)wst[child] + rank;
+      const int64_t wd = (int64_t)wc + rank;
 #pragma unroll
       for (int j = 0; j < D; ++j) Xo[(int64_t)j * n + wd] = X[(int64_t)j * n + p];
       Io[wd] = id;
-      NIDo[wd] = child;
+      NIDo[wd] = r1.y + (f ? 0 : 1);
     }
   }
 }
@@ -763,6 +788,8 @@ ckd_status ensure_node_cap(BuildBufs& B, int64_t need, cudaStream_t s) {
   CKD_CUDA(grow(&B.nleft, B.cap, nc, s));
   CKD_CUDA(grow(&B.pbase, B.cap, nc, s));
   CKD_CUDA(grow(&B.wst, B.cap, nc, s));
+  CKD_CUDA(grow(&B.frec, B.cap, nc, s));
+  CKD_CUDA(grow(&B.srec, B.cap * 2, nc * 2, s));
   B.cap = nc;
   return CKD_OK;
 }
@@ -771,7 +798,7 @@ void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
                 B.nleft,  B.pbase,   B.wst,       B.act[0],   B.act[1],  B.nxt_cnt, B.nxt_off,
-                B.tile_sum, B.tile_off, B.scal, B.flags};
+                B.tile_sum, B.tile_off, B.scal, B.flags, B.frec, B.srec};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -925,10 +952,11 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
       k_seg_box<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], n, nw, B.keys);
       CKD_LAUNCH_CHECK();
     }
-    k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext);
+    k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext, B.wst,
+                                   B.frec);
     CKD_LAUNCH_CHECK();
-    k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.meta, B.mode, B.ext, B.wst, n, nw,
-                                B.tile_sum, B.pstart, B.pend, B.flags);
+    k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.frec, B.ext, n, nw, B.tile_sum, B.pstart,
+                                B.pend, B.flags);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
     k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off, B.wst,
@@ -936,12 +964,12 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
                                      B.nxt_cnt, B.scal + 1);
     CKD_LAUNCH_CHECK();
     CKD_TRY(scan_i64(B.nxt_cnt, B.nxt_off, m, s));
-    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.act[1 - alist], B.wst);
+    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.mode, B.ext, B.nleft, B.pbase,
+                                   B.act[1 - alist], B.wst, B.srec);
     CKD_LAUNCH_CHECK();
-    k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.meta, B.mode, B.ext,
-                                     B.tile_off, B.nleft, B.pbase, B.wst, B.flags, leaf, n, nw,
-                                     B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids,
-                                     B.scal + 1);
+    k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off, B.flags,
+                                     n, nw, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts,
+                                     t->ids, B.scal + 1);
     CKD_LAUNCH_CHECK();
     CKD_CUDA(cudaMemcpyAsync(level_tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
