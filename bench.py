@@ -590,6 +590,9 @@ def main():
     ap.add_argument("--tune", default="", help="comma list key=value of ckd_set_tuning knobs")
     ap.add_argument("--profile", action="store_true",
                     help="one build and the kNN steps only (for ncu captures)")
+    ap.add_argument("--build-only", action="store_true",
+                    help="warmup + steps builds of the workload's tree, nothing else (build "
+                         "profiling; prints one line with the build times, not a bench line)")
     args = ap.parse_args()
     if args.impl == "reference":
         if args.workload in FOREST_WORKLOADS or args.workload in MULTI_WORKLOADS or \
@@ -643,6 +646,23 @@ def main():
 
     # ---- build (device-resident input), Mpt/s
     Pd = torch.from_numpy(P).cuda()
+    if args.build_only:
+        stream = torch.cuda.current_stream()
+        times = []
+        for it in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            tree = kdtree.build_kdtree(Pd, leaf=leaf, boxsize=box)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+            tree.close()
+        ms = float(np.mean(times))
+        print(json.dumps({"mode": "build-only", "workload": name, "n": n, "leaf": leaf,
+                          "build_ms": ms, "build_mpts": n / ms / 1e3, "all_ms": times}))
+        return 0
     build_ms = []
     n_builds = 1 if args.profile else 3
     for it in range(n_builds):

@@ -137,7 +137,7 @@ __global__ void k_compact_roots(const double* __restrict__ X, const int32_t* __r
 // inside a warp chunk go straight to atomicMin/atomicMax; the first and last
 // run of every warp chunk are merged per block by thread 0.
 template <int D>
-__global__ void __launch_bounds__(kBT) k_seg_box(const double* __restrict__ X,
+__global__ void __launch_bounds__(kBT, 5) k_seg_box(const double* __restrict__ X,
                                                  const int32_t* __restrict__ NID,
                                                  int64_t n, int64_t nw,
                                                  unsigned long long* __restrict__ keys) {
