@@ -42,6 +42,8 @@ static std::atomic<int> g_order_mode{0};
 int query_order_mode() { return g_order_mode.load(std::memory_order_relaxed); }
 static std::atomic<int> g_mlp_tc{1};
 bool mlp_tensor_cores() { return g_mlp_tc.load(std::memory_order_relaxed) != 0; }
+static std::atomic<int> g_box_warp{1};
+bool box_warp_enabled() { return g_box_warp.load(std::memory_order_relaxed) != 0; }
 void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -472,6 +474,10 @@ ckd_status ckd_set_tuning(int key, int value) {
     case 7:
       if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "MLP inference path must be 0 or 1");
       g_mlp_tc.store(value);
+      return CKD_OK;
+    case 8:
+      if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "box kernel choice must be 0 or 1");
+      g_box_warp.store(value);
       return CKD_OK;
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");

@@ -322,6 +322,164 @@ __global__ void __launch_bounds__(128) k_box_lane(TreeView tv, const double* __r
   if (!FILL) counts[bi] = cnt;
 }
 
+// Warp-per-box search for small batches, where one lane per box would leave most
+// of the GPU idle and each box would pay one dependent load per visited node.
+// The warp expands the frontier of visited nodes one level at a time (every lane
+// tests one frontier node with the descent rule of :1296-1300, so a level costs
+// one dependent load), keeping the frontier in leaf order: children replace
+// their parent, left first, and leaves stay in place (stored as ~id).  The final
+// frontier lists the visited leaves in the order of the left-first depth-first
+// walk, so every row comes out in the reference's order.  A frontier that
+// outgrows its buffer falls back to a depth-first walk with a warp stack.
+constexpr int kBoxFront = 256;
+constexpr int64_t kBoxWarpMax = 32768;  // boxes per call up to which the warp kernel is used
+
+template <int D, bool FILL>
+__global__ void __launch_bounds__(128) k_box_warp(TreeView tv, const double* __restrict__ boxes,
+                                                  int64_t nb, int64_t* __restrict__ counts,
+                                                  const int64_t* __restrict__ offsets,
+                                                  int64_t* __restrict__ oidx,
+                                                  const int32_t* __restrict__ broot) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ int32_t front[4][2][kBoxFront];
+  __shared__ int32_t stk[4][kBoxLaneStack];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t bi = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+  if (bi >= nb) return;  // the whole warp leaves together
+  double lo[D], hi[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    lo[j] = boxes[bi * 2 * D + 2 * j];
+    hi[j] = boxes[bi * 2 * D + 2 * j + 1];
+  }
+  int64_t cnt = 0;
+  int64_t cur = FILL ? offsets[bi] : 0;
+  const int64_t cur_end = FILL ? offsets[bi + 1] : 0;
+  const int32_t root = broot ? broot[bi] : 0;
+  // points of one leaf, tested by the lanes and emitted in position order
+  auto scan_leaf = [&](int32_t st, int32_t ct) {
+    for (int32_t b = 0; b < ct; b += 32) {
+      const int32_t p = st + b + lane;
+      bool in = b + lane < ct;
+      if (in) {
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          const double x = __ldg(&tv.pts[(int64_t)j * tv.n + p]);
+          in = in && !(x < lo[j] || x > hi[j]);  // :1319
+        }
+      }
+      const unsigned hm = __ballot_sync(FULL, in);
+      if (FILL) {
+        if (in) {
+          const int64_t o = cur + __popc(hm & lt);
+          if (o < cur_end) oidx[o] = __ldg(&tv.ids[p]);
+        }
+        cur += __popc(hm);
+      } else {
+        cnt += __popc(hm);
+      }
+    }
+  };
+  int nf = 1, fb = 0;
+  if (lane == 0) front[w][0][0] = root;
+  __syncwarp();
+  bool overflow = false;
+  for (;;) {
+    bool any = false;
+    for (int c = lane; c < nf; c += 32) any = any || front[w][fb][c] >= 0;
+    if (!__any_sync(FULL, any)) break;
+    int nn = 0;
+    for (int c0 = 0; c0 < nf; c0 += 32) {
+      const int c = c0 + lane;
+      int32_t o0 = 0, o1 = 0;
+      int kout = 0;
+      if (c < nf) {
+        const int32_t e = front[w][fb][c];
+        if (e < 0) {
+          o0 = e;
+          kout = 1;
+        } else {
+          const NodeMeta m = load_meta(tv.meta, e);
+          if (m.left < 0) {
+            o0 = ~e;
+            kout = 1;
+          } else {
+            double bl = 0.0, bh = 0.0;
+#pragma unroll
+            for (int j = 0; j < D; ++j)
+              if (j == m.axis) {
+                bl = lo[j];
+                bh = hi[j];
+              }
+            const bool gl = bl < m.split, gr = bh > m.split;  // :1296, :1300
+            o0 = gl ? m.left : m.left + 1;
+            o1 = m.left + 1;
+            kout = (gl ? 1 : 0) + (gr ? 1 : 0);
+          }
+        }
+      }
+      const unsigned b1 = __ballot_sync(FULL, kout >= 1), b2 = __ballot_sync(FULL, kout == 2);
+      const int pre = __popc(b1 & lt) + __popc(b2 & lt);
+      const int tot = __popc(b1) + __popc(b2);
+      if (nn + tot <= kBoxFront) {
+        if (kout >= 1) front[w][1 - fb][nn + pre] = o0;
+        if (kout == 2) front[w][1 - fb][nn + pre + 1] = o1;
+      }
+      nn += tot;
+    }
+    __syncwarp();
+    if (nn > kBoxFront) {
+      overflow = true;
+      break;
+    }
+    nf = nn;
+    fb = 1 - fb;
+  }
+  if (!overflow) {
+    for (int c0 = 0; c0 < nf; c0 += 32) {
+      int32_t st_l = 0, ct_l = 0;
+      if (c0 + lane < nf) {
+        const NodeMeta m = load_meta(tv.meta, ~front[w][fb][c0 + lane]);
+        st_l = m.start;
+        ct_l = m.count;
+      }
+      const int nl = min(32, nf - c0);
+      for (int i = 0; i < nl; ++i)
+        scan_leaf(__shfl_sync(FULL, st_l, i), __shfl_sync(FULL, ct_l, i));
+    }
+  } else {  // depth-first walk, left child first (stack depth <= tree depth + 2)
+    int top = 0;
+    if (lane == 0) stk[w][0] = root;
+    __syncwarp();
+    while (top >= 0) {
+      const int32_t node = stk[w][top];
+      --top;
+      __syncwarp();
+      const NodeMeta m = load_meta(tv.meta, node);
+      if (m.left < 0) {
+        scan_leaf(m.start, m.count);
+      } else {
+        double bl = 0.0, bh = 0.0;
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          if (j == m.axis) {
+            bl = lo[j];
+            bh = hi[j];
+          }
+        const bool gr = bh > m.split, gl = bl < m.split;
+        if (lane == 0) {
+          if (gr) stk[w][top + 1] = m.left + 1;
+          if (gl) stk[w][top + 1 + (gr ? 1 : 0)] = m.left;
+        }
+        top += (gr ? 1 : 0) + (gl ? 1 : 0);
+        __syncwarp();
+      }
+    }
+  }
+  if (!FILL && lane == 0) counts[bi] = cnt;
+}
+
 template <int D, bool FILL>
 __global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restrict__ boxes,
                                              int64_t nb, int32_t* __restrict__ gstack,
@@ -480,6 +638,15 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
                       const int32_t* broot) {
   TreeView tv = t->view();
   const int threads = 128, nw = threads / 32;
+  if (t->depth < kBoxLaneStack - 2 && nb <= kBoxWarpMax && box_warp_enabled()) {
+    const unsigned wb = (unsigned)cdiv(nb, nw);
+    if (fill)
+      k_box_warp<D, true><<<wb, threads, 0, s>>>(tv, boxes, nb, nullptr, offsets, idx, broot);
+    else
+      k_box_warp<D, false><<<wb, threads, 0, s>>>(tv, boxes, nb, counts, nullptr, nullptr, broot);
+    CKD_LAUNCH_CHECK();
+    return CKD_OK;
+  }
   if (t->depth < kBoxLaneStack - 2) {
     const unsigned lb = (unsigned)cdiv(nb, threads);
     if (fill)

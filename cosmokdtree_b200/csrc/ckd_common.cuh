@@ -52,6 +52,7 @@ int gather_warps_per_block();
 int query_order_mode();
 // learned-bound network inference on the tensor cores (tcgen05) instead of FP32 FMAs
 bool mlp_tensor_cores();
+bool box_warp_enabled();
 
 // events bracketing the main search kernel when kernel timing is on
 void timing_begin(cudaStream_t s);

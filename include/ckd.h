@@ -124,7 +124,9 @@ ckd_status ckd_set_knn_variant(int variant);
  * key 5: warps per block of the warp-gather kernel (1..4, default 2);
  * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
  * default; 1 = always; 2 = never); key 7: inference of the learned-bound network
- * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations, default). */
+ * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations, default);
+ * key 8: box search of up to 32768 boxes per call (1 = a warp per box, frontier
+ * expanded a level at a time, default; 0 = a lane per box). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference

@@ -199,6 +199,34 @@ def test_gpu_box_matches_oracle(gpu, oracle):
     np.testing.assert_array_equal(one, oi[oo[1]:oo[2]])
 
 
+@pytest.mark.parametrize("warp", [0, 1])
+def test_gpu_box_kernels_match_oracle(gpu, oracle, warp):
+    """Both box kernels (a lane per box; a warp per box with the level-wise
+    frontier and its depth-first fallback for boxes over many leaves), on a
+    forest-free tree, small and large batches (the warp kernel serves up to 32768
+    boxes per call)."""
+    from cosmokdtree_b200 import _lib
+    P = make_points("clustered_dup", 60000, 3, True)
+    rng = np.random.default_rng(16)
+    nb = 40000 if warp == 0 else 3000
+    lo = rng.random((nb, 3)) - 0.55
+    B = np.empty((nb, 6))
+    B[:, 0::2] = lo
+    B[:, 1::2] = lo + rng.choice([0.01, 0.05, 0.3], (nb, 1)) * rng.random((nb, 3))
+    B[:5] = [-0.5, 0.5, -0.5, 0.5, -0.5, 0.5]  # every leaf: frontier overflow
+    t = gpu.kdtree.build_kdtree(P, boxsize=1.0)
+    ot = oracle.OracleTree(P, 16, 1.0)
+    L = _lib.load()
+    _lib.check(L.ckd_set_tuning(8, warp))
+    try:
+        xo, xi = (_np(x) for x in gpu.kdtree.box_search_csr(t, B))
+    finally:
+        _lib.check(L.ckd_set_tuning(8, 1))
+    oo, oi = ot.box_csr(B)
+    np.testing.assert_array_equal(xo, oo)
+    np.testing.assert_array_equal(xi, oi)
+
+
 def test_gpu_box_on_split_plane_quirk(gpu, oracle):
     """A point lying exactly on a split plane is missed when box_hi == split
     (strict descent, cosmokdtree.f90:1296-1300); the GPU reproduces the rule."""
