@@ -98,56 +98,154 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
   if (!FILL && valid) counts[qi] = cnt;
 }
 
+__device__ __forceinline__ bool key_lt(double d1, int64_t i1, double d2, int64_t i2) {
+  return d1 < d2 || (d1 == d2 && i1 < i2);
+}
+
 // Per-row sort by (d2, id) of the fill output (d2 stored in dist), then sqrt.
-// Insertion sort for short rows, heap sort otherwise.
+// Rows of at most 32 results: insertion sort by their own thread.  Longer rows
+// are listed for k_sort_big (a block per row), with a scratch range for the
+// rows longer than one shared-memory tile.
+constexpr int kSortTile = 2048;
 __global__ void k_sort_rows(const int64_t* __restrict__ offsets, int64_t nq,
-                            int64_t* __restrict__ idx, double* __restrict__ dist) {
+                            int64_t* __restrict__ idx, double* __restrict__ dist,
+                            int32_t* __restrict__ big, unsigned long long* __restrict__ sel,
+                            int64_t* __restrict__ tmp_off) {
   int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (qi >= nq) return;
   int64_t b = offsets[qi], e = offsets[qi + 1], n = e - b;
+  if (n > 32) {
+    const unsigned long long slot = atomicAdd(&sel[0], 1ull);
+    big[slot] = (int32_t)qi;
+    tmp_off[slot] = n > kSortTile ? (int64_t)atomicAdd(&sel[1], (unsigned long long)n) : 0;
+    return;
+  }
   double* D2 = dist + b;
   int64_t* I = idx + b;
-  auto lt = [](double d1, int64_t i1, double d2, int64_t i2) {
-    return d1 < d2 || (d1 == d2 && i1 < i2);
-  };
-  if (n <= 32) {
-    for (int64_t i = 1; i < n; ++i) {
-      double d = D2[i];
-      int64_t x = I[i];
-      int64_t j = i - 1;
-      while (j >= 0 && lt(d, x, D2[j], I[j])) {
-        D2[j + 1] = D2[j];
-        I[j + 1] = I[j];
-        --j;
-      }
-      D2[j + 1] = d;
-      I[j + 1] = x;
+  for (int64_t i = 1; i < n; ++i) {
+    double d = D2[i];
+    int64_t x = I[i];
+    int64_t j = i - 1;
+    while (j >= 0 && key_lt(d, x, D2[j], I[j])) {
+      D2[j + 1] = D2[j];
+      I[j + 1] = I[j];
+      --j;
     }
-  } else {
-    auto sift = [&](int64_t i, int64_t end, double d, int64_t x) {
-      for (;;) {
-        int64_t l = 2 * i + 1;
-        if (l >= end) break;
-        int64_t c = l;
-        if (l + 1 < end && lt(D2[l], I[l], D2[l + 1], I[l + 1])) c = l + 1;
-        if (!lt(d, x, D2[c], I[c])) break;
-        D2[i] = D2[c];
-        I[i] = I[c];
-        i = c;
-      }
-      D2[i] = d;
-      I[i] = x;
-    };
-    for (int64_t i = n / 2 - 1; i >= 0; --i) sift(i, n, D2[i], I[i]);
-    for (int64_t end = n - 1; end > 0; --end) {
-      double d = D2[end];
-      int64_t x = I[end];
-      D2[end] = D2[0];
-      I[end] = I[0];
-      sift(0, end, d, x);
-    }
+    D2[j + 1] = d;
+    I[j + 1] = x;
   }
   for (int64_t i = 0; i < n; ++i) D2[i] = sqrt(D2[i]);
+}
+
+// A block per listed row: tiles of kSortTile sorted in shared memory (bitonic),
+// then merge passes of doubling width between the row and its scratch range
+// (merge path: each thread finds where its 8 outputs start by binary search).
+// Keys (d2, id) are distinct within a row, so the order is total.
+__global__ void __launch_bounds__(256) k_sort_big(const int64_t* __restrict__ offsets,
+                                                  const int32_t* __restrict__ big,
+                                                  const unsigned long long* __restrict__ sel,
+                                                  const int64_t* __restrict__ tmp_off,
+                                                  int64_t* __restrict__ idx,
+                                                  double* __restrict__ dist,
+                                                  int64_t* __restrict__ tidx,
+                                                  double* __restrict__ tdist) {
+  __shared__ double sk[kSortTile];
+  __shared__ int64_t si[kSortTile];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int64_t nbig = (int64_t)sel[0];
+  for (int64_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+    const int32_t qi = big[r];
+    const int64_t b = offsets[qi], n = offsets[qi + 1] - b;
+    double* D2 = dist + b;
+    int64_t* I = idx + b;
+    for (int64_t t0 = 0; t0 < n; t0 += kSortTile) {
+      const int m = (int)min((int64_t)kSortTile, n - t0);
+      int P = 1;
+      while (P < m) P <<= 1;
+      for (int i = tid; i < P; i += nt) {
+        sk[i] = i < m ? D2[t0 + i] : INFINITY;
+        si[i] = i < m ? I[t0 + i] : INT64_MAX;
+      }
+      __syncthreads();
+      for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = tid; i < P; i += nt) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const bool up = (i & k) == 0;
+              if (key_lt(sk[ixj], si[ixj], sk[i], si[i]) == up) {
+                const double td = sk[i];
+                const int64_t ti = si[i];
+                sk[i] = sk[ixj];
+                si[i] = si[ixj];
+                sk[ixj] = td;
+                si[ixj] = ti;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = tid; i < m; i += nt) {
+        D2[t0 + i] = sk[i];
+        I[t0 + i] = si[i];
+      }
+      __syncthreads();
+    }
+    if (n > kSortTile) {
+      double* sD = D2;
+      int64_t* sI = I;
+      double* dD = tdist + tmp_off[r];
+      int64_t* dI = tidx + tmp_off[r];
+      for (int64_t w = kSortTile; w < n; w <<= 1) {
+        for (int64_t s0 = 0; s0 < n; s0 += 2 * w) {
+          const int64_t na = min(w, n - s0);
+          const int64_t nb = max((int64_t)0, min(w, n - s0 - w));
+          const double* AD = sD + s0;
+          const int64_t* AI = sI + s0;
+          const double* BD = AD + na;
+          const int64_t* BI = AI + na;
+          const int64_t mt = na + nb;
+          for (int64_t k0 = (int64_t)tid * 8; k0 < mt; k0 += (int64_t)nt * 8) {
+            int64_t lo = max((int64_t)0, k0 - nb), hi = min(k0, na);
+            while (lo < hi) {
+              const int64_t mid = (lo + hi) >> 1;
+              if (key_lt(AD[mid], AI[mid], BD[k0 - 1 - mid], BI[k0 - 1 - mid])) lo = mid + 1;
+              else hi = mid;
+            }
+            int64_t i = lo, j = k0 - lo;
+            const int64_t kend = min(k0 + 8, mt);
+            for (int64_t k = k0; k < kend; ++k) {
+              const bool ta = j >= nb || (i < na && key_lt(AD[i], AI[i], BD[j], BI[j]));
+              if (ta) {
+                dD[s0 + k] = AD[i];
+                dI[s0 + k] = AI[i];
+                ++i;
+              } else {
+                dD[s0 + k] = BD[j];
+                dI[s0 + k] = BI[j];
+                ++j;
+              }
+            }
+          }
+        }
+        __syncthreads();
+        double* tD = sD;
+        sD = dD;
+        dD = tD;
+        int64_t* tI = sI;
+        sI = dI;
+        dI = tI;
+      }
+      if (sD != D2)
+        for (int64_t i = tid; i < n; i += nt) {
+          D2[i] = sD[i];
+          I[i] = sI[i];
+        }
+      __syncthreads();
+    }
+    for (int64_t i = tid; i < n; i += nt) D2[i] = sqrt(D2[i]);
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------- heavy ball rows
@@ -161,6 +259,19 @@ __global__ void k_sort_rows(const int64_t* __restrict__ offsets, int64_t nq,
 constexpr int64_t kHeavyRow = 256;
 constexpr int kHeavyStack = 128;
 
+// A whole subtree of at least kTaskMin points inside a heavy row's ball is not
+// copied by the warp that found it but recorded as emission tasks of at most
+// kTaskChunk points, which k_ball_emit spreads over the whole GPU: a row of
+// millions of points no longer serialises on one warp.  When the task buffer is
+// full the warp copies the subtree itself (same output).
+constexpr int32_t kTaskMin = 1024;
+constexpr int32_t kTaskChunk = 4096;
+constexpr unsigned kTaskCap = 1u << 20;
+struct EmitTask {
+  int64_t out;  // first output slot
+  int32_t start, count, qi, pad;
+};
+
 template <int D, bool PER>
 __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const double* __restrict__ Q,
                                                         const int32_t* __restrict__ rows,
@@ -169,7 +280,9 @@ __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const doubl
                                                         int stack_len,
                                                         const int64_t* __restrict__ offsets,
                                                         int64_t* __restrict__ oidx,
-                                                        double* __restrict__ odist, int want_d2) {
+                                                        double* __restrict__ odist, int want_d2,
+                                                        EmitTask* __restrict__ tasks,
+                                                        unsigned* __restrict__ n_tasks) {
   __shared__ int32_t sstk[4][kHeavyStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -193,6 +306,26 @@ __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const doubl
       if (!(box_mind2<D, PER>(tv, q, node) <= r2)) continue;
       const bool inside =
           m.left >= 0 && (PER ? box_maxd2_near<D>(tv, q, node) : box_maxd2<D>(tv, q, node)) <= r2;
+      if (inside && tasks && m.count >= kTaskMin && cur < cur_end) {
+        const int64_t len = min((int64_t)m.count, cur_end - cur);
+        const unsigned nt = (unsigned)((len + kTaskChunk - 1) / kTaskChunk);
+        unsigned tb = 0;
+        if (lane == 0) tb = atomicAdd(n_tasks, nt);
+        tb = __shfl_sync(0xffffffffu, tb, 0);
+        if (tb + nt <= kTaskCap) {
+          for (unsigned c = lane; c < nt; c += 32) {
+            EmitTask e;
+            e.out = cur + (int64_t)c * kTaskChunk;
+            e.start = m.start + (int32_t)c * kTaskChunk;
+            e.count = (int32_t)min((int64_t)kTaskChunk, len - (int64_t)c * kTaskChunk);
+            e.qi = (int32_t)qi;
+            e.pad = 0;
+            tasks[tb + c] = e;
+          }
+          cur += m.count;
+          continue;
+        }
+      }
       if (inside) {  // whole subtree: positions m.start .. m.start + count - 1 in order
         for (int32_t i = lane; i < m.count; i += 32) {
           const int32_t p = m.start + i;
@@ -233,6 +366,32 @@ __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const doubl
       }
     }
     __syncwarp();
+  }
+}
+
+// Copies of the recorded whole-subtree chunks, a warp per chunk.
+template <int D, bool PER>
+__global__ void __launch_bounds__(128) k_ball_emit(TreeView tv, const double* __restrict__ Q,
+                                                   const EmitTask* __restrict__ tasks,
+                                                   const unsigned* __restrict__ n_tasks,
+                                                   int64_t* __restrict__ oidx,
+                                                   double* __restrict__ odist, int want_d2) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nt = min((int64_t)*n_tasks, (int64_t)kTaskCap);
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < nt;
+       t += nwarps) {
+    const EmitTask e = tasks[t];
+    double q[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) q[j] = Q[(int64_t)e.qi * D + j];
+#pragma unroll 4
+    for (int32_t i = lane; i < e.count; i += 32) {
+      const int32_t p = e.start + i;
+      const double d2 = point_d2<D, PER>(tv, q, p);
+      oidx[e.out + i] = __ldg(&tv.ids[p]);
+      odist[e.out + i] = want_d2 ? d2 : sqrt(d2);
+    }
   }
 }
 
@@ -614,10 +773,21 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     const int hstack_len = std::max(kHeavyStack, t->depth + 4);
     if (hstack_len > kHeavyStack)
       CKD_CUDA(dev_alloc((void**)&hstack, sizeof(int32_t) * hstack_len * hblocks * 4, s));
+    EmitTask* tasks = nullptr;
+    unsigned* ntask = nullptr;
+    CKD_CUDA(dev_alloc((void**)&tasks, sizeof(EmitTask) * kTaskCap, s));
+    CKD_CUDA(dev_alloc((void**)&ntask, sizeof(unsigned), s));
+    CKD_CUDA(cudaMemsetAsync(ntask, 0, sizeof(unsigned), s));
     k_ball_fill_warp<D, PER><<<(unsigned)std::max<int64_t>(1, hblocks), 128, 0, s>>>(
-        tv, q, heavy, cnt, r2, hstack, hstack_len, offsets, idx, dist, sorted ? 1 : 0);
+        tv, q, heavy, cnt, r2, hstack, hstack_len, offsets, idx, dist, sorted ? 1 : 0, tasks,
+        ntask);
     CKD_LAUNCH_CHECK();
-    for (void* p : {(void*)heavy, (void*)light, (void*)cnt, (void*)hstack}) dev_free(p, s);
+    k_ball_emit<D, PER><<<(unsigned)sms * 8, 128, 0, s>>>(tv, q, tasks, ntask, idx, dist,
+                                                          sorted ? 1 : 0);
+    CKD_LAUNCH_CHECK();
+    for (void* p : {(void*)heavy, (void*)light, (void*)cnt, (void*)hstack, (void*)tasks,
+                    (void*)ntask})
+      dev_free(p, s);
   } else {
     k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2, gstack,
                                                       stack_len, counts, nullptr, nullptr, nullptr,
@@ -625,8 +795,35 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     CKD_LAUNCH_CHECK();
   }
   if (fill && sorted) {
-    k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist);
+    int32_t* big = nullptr;
+    int64_t* toff = nullptr;
+    unsigned long long* sel = nullptr;
+    CKD_CUDA(dev_alloc((void**)&big, sizeof(int32_t) * nq, s));
+    CKD_CUDA(dev_alloc((void**)&toff, sizeof(int64_t) * nq, s));
+    CKD_CUDA(dev_alloc((void**)&sel, 2 * sizeof(unsigned long long), s));
+    CKD_CUDA(cudaMemsetAsync(sel, 0, 2 * sizeof(unsigned long long), s));
+    k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist, big, sel, toff);
     CKD_LAUNCH_CHECK();
+    unsigned long long hs[2] = {0, 0};
+    CKD_CUDA(cudaMemcpyAsync(hs, sel, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    CKD_CUDA(cudaStreamSynchronize(s));
+    if (hs[0] > 0) {
+      int64_t* tidx = nullptr;
+      double* tdist = nullptr;
+      if (hs[1] > 0) {
+        CKD_CUDA(dev_alloc((void**)&tidx, sizeof(int64_t) * hs[1], s));
+        CKD_CUDA(dev_alloc((void**)&tdist, sizeof(double) * hs[1], s));
+      }
+      int dev = 0, sms = 148;
+      CKD_CUDA(cudaGetDevice(&dev));
+      CKD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      const unsigned g = (unsigned)std::min<unsigned long long>(hs[0], (unsigned long long)sms * 8);
+      k_sort_big<<<g, 256, 0, s>>>(offsets, big, sel, toff, idx, dist, tidx, tdist);
+      CKD_LAUNCH_CHECK();
+      dev_free(tidx, s);
+      dev_free(tdist, s);
+    }
+    for (void* p : {(void*)big, (void*)toff, (void*)sel}) dev_free(p, s);
   }
   if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;

@@ -181,6 +181,30 @@ def test_gpu_ball_matches_oracle(gpu, oracle, periodic, sorted_):
             np.testing.assert_array_equal(np.sort(il[j]), np.sort(ref))
 
 
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("sorted_", [False, True])
+def test_gpu_ball_heavy_rows_match_oracle(gpu, oracle, periodic, sorted_):
+    """Rows of tens of thousands of results: whole subtrees go through the
+    emission tasks, sorted rows through the block merge sort."""
+    P = make_points("clustered", 120000, 3, periodic, seed=3)
+    rng = np.random.default_rng(8)
+    Q = np.concatenate([P[rng.integers(0, len(P), 40)], rng.random((10, 3)) - 0.5])
+    box = 1.0 if periodic else None
+    t = gpu.kdtree.build_kdtree(P, boxsize=box)
+    ot = oracle.OracleTree(P, 16, box)
+    r = 0.25
+    off, idx, dist = (_np(x) for x in gpu.kdtree.ball_search_csr(t, Q, r, sorted=sorted_))
+    ooff, oidx, odist = ot.ball_csr(Q, r, sorted=sorted_)
+    np.testing.assert_array_equal(off, ooff)
+    assert np.diff(off).max() > 8192  # several shared-memory tiles per long row
+    if sorted_ or not periodic:
+        np.testing.assert_array_equal(idx, oidx)
+        np.testing.assert_array_equal(dist, odist)
+    else:
+        for a, b in zip(_rows(off, idx), _rows(ooff, oidx)):
+            np.testing.assert_array_equal(np.sort(a), np.sort(b))
+
+
 def test_gpu_box_matches_oracle(gpu, oracle):
     P = make_points("clustered_dup", 50000, 3, False)
     rng = np.random.default_rng(6)
