@@ -92,6 +92,10 @@ SIGNATURES = {
     "ckd_ball_fill": [_vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],
     "ckd_box_count": [_vp, _vp, _i64, _vp, _vp],
     "ckd_box_fill": [_vp, _vp, _i64, _vp, _vp, _vp],
+    "ckd_ball_count_host": [_vp, _vp, _i64, _dbl, _vp, _vp],
+    "ckd_ball_fill_host": [_vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],
+    "ckd_box_count_host": [_vp, _vp, _i64, _vp, _vp],
+    "ckd_box_fill_host": [_vp, _vp, _i64, _vp, _vp, _vp],
     "ckd_exclusive_scan": [_vp, _vp, _i64, _vp],
     "ckd_tree_save": [_vp, ctypes.c_char_p],
     "ckd_tree_load": [ctypes.c_char_p, ctypes.POINTER(_vp)],

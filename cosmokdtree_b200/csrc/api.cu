@@ -575,6 +575,141 @@ ckd_status ckd_box_fill(const ckd_tree* t, const double* boxes, int64_t nb, cons
   return box_run(t, boxes, nb, true, nullptr, offsets, idx, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------- two-phase CSR on host buffers
+// For callers without device memory of their own (Fortran, C, other FFIs): the
+// count phase returns the CSR offsets in host memory, the caller allocates the
+// rows and the fill phase writes them.  Both phases are synchronous.
+namespace {
+struct DevScratch {
+  cudaStream_t s;
+  std::vector<void*> ps;
+  void* get(size_t bytes, cudaError_t& e) {
+    void* p = nullptr;
+    e = dev_alloc(&p, bytes, s);
+    if (e == cudaSuccess) ps.push_back(p);
+    return p;
+  }
+  ~DevScratch() {
+    for (void* p : ps) dev_free(p, s);
+    cudaStreamSynchronize(s);
+  }
+};
+
+ckd_status offsets_to_host(const int64_t* counts, int64_t n, int64_t* offsets_host,
+                           DevScratch& sc) {
+  cudaError_t e;
+  int64_t* off = (int64_t*)sc.get(sizeof(int64_t) * (n + 1), e);
+  CKD_CUDA(e);
+  CKD_TRY(scan_i64(counts, off, n, sc.s));
+  CKD_CUDA(cudaMemcpyAsync(offsets_host, off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                           sc.s));
+  CKD_CUDA(cudaStreamSynchronize(sc.s));
+  return CKD_OK;
+}
+}  // namespace
+
+ckd_status ckd_ball_count_host(const ckd_tree* t, const double* q, int64_t nq, double radius,
+                               int64_t* offsets_host, void* stream) {
+  CKD_TRY(check_single(t));
+  if (!(radius > 0) || !std::isfinite(radius))
+    return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (!offsets_host) return fail(CKD_ERR_BAD_ARG, "null offsets pointer");
+  offsets_host[0] = 0;
+  if (nq == 0) return CKD_OK;
+  if (!q) return fail(CKD_ERR_BAD_ARG, "null query pointer");
+  DevScratch sc{(cudaStream_t)stream, {}};
+  cudaError_t e;
+  double* dq = (double*)sc.get(sizeof(double) * nq * t->d, e);
+  CKD_CUDA(e);
+  int64_t* cnt = (int64_t*)sc.get(sizeof(int64_t) * nq, e);
+  CKD_CUDA(e);
+  CKD_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * nq * t->d, cudaMemcpyHostToDevice, sc.s));
+  CKD_TRY(ball_run(t, dq, nq, radius, false, 0, cnt, nullptr, nullptr, nullptr, sc.s));
+  return offsets_to_host(cnt, nq, offsets_host, sc);
+}
+
+ckd_status ckd_ball_fill_host(const ckd_tree* t, const double* q, int64_t nq, double radius,
+                              int sorted, const int64_t* offsets_host, int64_t* idx_host,
+                              double* dist_host, void* stream) {
+  CKD_TRY(check_single(t));
+  if (!(radius > 0) || !std::isfinite(radius))
+    return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !offsets_host) return fail(CKD_ERR_BAD_ARG, "null query or offsets pointer");
+  const int64_t total = offsets_host[nq];
+  if (total < 0) return fail(CKD_ERR_BAD_ARG, "negative result count");
+  if (total > 0 && (!idx_host || !dist_host)) return fail(CKD_ERR_BAD_ARG, "null output pointer");
+  DevScratch sc{(cudaStream_t)stream, {}};
+  cudaError_t e;
+  double* dq = (double*)sc.get(sizeof(double) * nq * t->d, e);
+  CKD_CUDA(e);
+  int64_t* off = (int64_t*)sc.get(sizeof(int64_t) * (nq + 1), e);
+  CKD_CUDA(e);
+  int64_t* di = (int64_t*)sc.get(sizeof(int64_t) * std::max<int64_t>(total, 1), e);
+  CKD_CUDA(e);
+  double* dd = (double*)sc.get(sizeof(double) * std::max<int64_t>(total, 1), e);
+  CKD_CUDA(e);
+  CKD_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * nq * t->d, cudaMemcpyHostToDevice, sc.s));
+  CKD_CUDA(cudaMemcpyAsync(off, offsets_host, sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice,
+                           sc.s));
+  if (total > 0) {
+    CKD_TRY(ball_run(t, dq, nq, radius, true, sorted, nullptr, off, di, dd, sc.s));
+    CKD_CUDA(cudaMemcpyAsync(idx_host, di, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, sc.s));
+    CKD_CUDA(cudaMemcpyAsync(dist_host, dd, sizeof(double) * total, cudaMemcpyDeviceToHost, sc.s));
+  }
+  CKD_CUDA(cudaStreamSynchronize(sc.s));
+  return CKD_OK;
+}
+
+ckd_status ckd_box_count_host(const ckd_tree* t, const double* boxes, int64_t nb,
+                              int64_t* offsets_host, void* stream) {
+  CKD_TRY(check_single(t));
+  if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
+  if (!offsets_host) return fail(CKD_ERR_BAD_ARG, "null offsets pointer");
+  offsets_host[0] = 0;
+  if (nb == 0) return CKD_OK;
+  if (!boxes) return fail(CKD_ERR_BAD_ARG, "null box pointer");
+  DevScratch sc{(cudaStream_t)stream, {}};
+  cudaError_t e;
+  double* db = (double*)sc.get(sizeof(double) * nb * 2 * t->d, e);
+  CKD_CUDA(e);
+  int64_t* cnt = (int64_t*)sc.get(sizeof(int64_t) * nb, e);
+  CKD_CUDA(e);
+  CKD_CUDA(cudaMemcpyAsync(db, boxes, sizeof(double) * nb * 2 * t->d, cudaMemcpyHostToDevice, sc.s));
+  CKD_TRY(box_run(t, db, nb, false, cnt, nullptr, nullptr, sc.s));
+  return offsets_to_host(cnt, nb, offsets_host, sc);
+}
+
+ckd_status ckd_box_fill_host(const ckd_tree* t, const double* boxes, int64_t nb,
+                             const int64_t* offsets_host, int64_t* idx_host, void* stream) {
+  CKD_TRY(check_single(t));
+  if (nb < 0) return fail(CKD_ERR_BAD_ARG, "negative box count");
+  if (nb == 0) return CKD_OK;
+  if (!boxes || !offsets_host) return fail(CKD_ERR_BAD_ARG, "null box or offsets pointer");
+  const int64_t total = offsets_host[nb];
+  if (total < 0) return fail(CKD_ERR_BAD_ARG, "negative result count");
+  if (total > 0 && !idx_host) return fail(CKD_ERR_BAD_ARG, "null output pointer");
+  DevScratch sc{(cudaStream_t)stream, {}};
+  cudaError_t e;
+  double* db = (double*)sc.get(sizeof(double) * nb * 2 * t->d, e);
+  CKD_CUDA(e);
+  int64_t* off = (int64_t*)sc.get(sizeof(int64_t) * (nb + 1), e);
+  CKD_CUDA(e);
+  int64_t* di = (int64_t*)sc.get(sizeof(int64_t) * std::max<int64_t>(total, 1), e);
+  CKD_CUDA(e);
+  CKD_CUDA(cudaMemcpyAsync(db, boxes, sizeof(double) * nb * 2 * t->d, cudaMemcpyHostToDevice, sc.s));
+  CKD_CUDA(cudaMemcpyAsync(off, offsets_host, sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice,
+                           sc.s));
+  if (total > 0) {
+    CKD_TRY(box_run(t, db, nb, true, nullptr, off, di, sc.s));
+    CKD_CUDA(cudaMemcpyAsync(idx_host, di, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, sc.s));
+  }
+  CKD_CUDA(cudaStreamSynchronize(sc.s));
+  return CKD_OK;
+}
+
 ckd_status ckd_exclusive_scan(const int64_t* in, int64_t* out, int64_t n, void* stream) {
   if (n < 0 || !out || (n > 0 && !in)) return fail(CKD_ERR_BAD_ARG, "bad scan arguments");
   return scan_i64(in, out, n, (cudaStream_t)stream);

@@ -185,6 +185,22 @@ ckd_status ckd_box_count(const ckd_tree* tree, const double* boxes_dev, int64_t 
 ckd_status ckd_box_fill(const ckd_tree* tree, const double* boxes_dev, int64_t nb,
                         const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
 
+/* The same two-phase protocols on host buffers, for callers without device
+ * memory of their own (the Fortran module cosmokdtree_gpu, C, other FFIs); the
+ * shape of pyball_search_call_1/2 and pybox_search_call_1/2
+ * (src/cosmokdtree2py.f90:153-315) with caller-owned rows.  Phase 1 writes the
+ * CSR offsets (offsets_host[n+1], n = nq or nb); the caller allocates
+ * offsets_host[n] results; phase 2 fills them.  Ids are 0-based.  Synchronous. */
+ckd_status ckd_ball_count_host(const ckd_tree* tree, const double* q_host, int64_t nq,
+                               double radius, int64_t* offsets_host, void* stream);
+ckd_status ckd_ball_fill_host(const ckd_tree* tree, const double* q_host, int64_t nq,
+                              double radius, int sorted, const int64_t* offsets_host,
+                              int64_t* idx_host, double* dist_host, void* stream);
+ckd_status ckd_box_count_host(const ckd_tree* tree, const double* boxes_host, int64_t nb,
+                              int64_t* offsets_host, void* stream);
+ckd_status ckd_box_fill_host(const ckd_tree* tree, const double* boxes_host, int64_t nb,
+                             const int64_t* offsets_host, int64_t* idx_host, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Forests: many independent trees of uneven sizes built and searched together
  * (halo / subvolume catalogues).  No single-call counterpart in the reference,

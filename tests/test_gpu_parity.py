@@ -373,3 +373,46 @@ def test_gpu_pool_reuse_and_release(gpu):
         np.testing.assert_array_equal(e[key], ref[key])
     d, i = kd.knn_search(t, P[:5], 3)
     assert (i[:, 0] == np.arange(5)).all()
+
+
+def test_gpu_host_csr_entry_points(gpu, oracle):
+    """The host-buffer two-phase ball and box entry points (used by the Fortran
+    front end) give the device path's CSR."""
+    import ctypes
+    from cosmokdtree_b200 import _lib
+    L = _lib.load()
+    P = make_points("clustered", 30000, 3, True, seed=4)
+    rng = np.random.default_rng(21)
+    Q = np.ascontiguousarray(np.concatenate([P[:200], rng.random((100, 3)) - 0.5]))
+    t = gpu.kdtree.build_kdtree(P, boxsize=1.0)
+    ot = oracle.OracleTree(P, 16, 1.0)
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data)
+    for sorted_ in (0, 1):
+        off = np.empty(len(Q) + 1, np.int64)
+        _lib.check(L.ckd_ball_count_host(t.handle, vp(Q), len(Q), 0.02, vp(off), None))
+        idx = np.empty(max(off[-1], 1), np.int64)
+        dist = np.empty(max(off[-1], 1), np.float64)
+        _lib.check(L.ckd_ball_fill_host(t.handle, vp(Q), len(Q), 0.02, sorted_, vp(off), vp(idx),
+                                        vp(dist), None))
+        ooff, oidx, odist = ot.ball_csr(Q, 0.02, sorted=bool(sorted_))
+        np.testing.assert_array_equal(off, ooff)
+        if sorted_:
+            np.testing.assert_array_equal(idx[:off[-1]], oidx)
+            np.testing.assert_array_equal(dist[:off[-1]], odist)
+        else:
+            for a, b in zip(_rows(off, idx), _rows(ooff, oidx)):
+                np.testing.assert_array_equal(np.sort(a), np.sort(b))
+    lo = rng.random((500, 3)) - 0.55
+    B = np.empty((500, 6))
+    B[:, 0::2] = lo
+    B[:, 1::2] = lo + 0.08 * rng.random((500, 3))
+    off = np.empty(len(B) + 1, np.int64)
+    _lib.check(L.ckd_box_count_host(t.handle, vp(B), len(B), vp(off), None))
+    idx = np.empty(max(off[-1], 1), np.int64)
+    _lib.check(L.ckd_box_fill_host(t.handle, vp(B), len(B), vp(off), vp(idx), None))
+    oo, oi = ot.box_csr(B)
+    np.testing.assert_array_equal(off, oo)
+    np.testing.assert_array_equal(idx[:off[-1]], oi)
+    empty = np.zeros(1, np.int64)
+    _lib.check(L.ckd_box_count_host(t.handle, vp(B), 0, vp(empty), None))
+    assert empty[0] == 0
