@@ -105,6 +105,8 @@ SIGNATURES = {
     "ckd_forest_knn": [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
     "ckd_forest_box_count": [_vp, _vp, _vp, _i64, _vp, _vp],
     "ckd_forest_box_fill": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],
+    "ckd_forest_ball_count": [_vp, _vp, _vp, _i64, _dbl, _vp, _vp],
+    "ckd_forest_ball_fill": [_vp, _vp, _vp, _i64, _dbl, _int, _vp, _vp, _vp, _vp],
     "ckd_mlp_create": [ctypes.c_uint64, ctypes.POINTER(_vp)],
     "ckd_mlp_free": [_vp],
     "ckd_mlp_get": [_vp, _vp, _vp, _vp, _vp],

@@ -118,7 +118,8 @@ ckd_status knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, i
                        int sorted, double* dist, int64_t* idx, int64_t* nfb, cudaStream_t s);
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
-                    cudaStream_t s);
+                    cudaStream_t s,
+                    const int32_t* qroot = nullptr);
 ckd_status box_run(const ckd_tree* t, const double* boxes, int64_t nb, bool fill, int64_t* counts,
                    const int64_t* offsets, int64_t* idx, cudaStream_t s,
                    const int32_t* broot = nullptr);
@@ -311,6 +312,40 @@ ckd_status ckd_forest_box_count(const ckd_tree* t, const double* boxes, const in
 ckd_status ckd_forest_box_fill(const ckd_tree* t, const double* boxes, const int64_t* b_offsets,
                                int64_t nb, const int64_t* offsets, int64_t* idx, void* stream) {
   return forest_box(t, boxes, b_offsets, nb, true, nullptr, offsets, idx, stream);
+}
+
+static ckd_status forest_ball(const ckd_tree* t, const double* q, const int64_t* q_offsets,
+                              int64_t nq, double radius, bool fill, int sorted, int64_t* counts,
+                              const int64_t* offsets, int64_t* idx, double* dist, void* stream) {
+  CKD_TRY(check_forest(t));
+  if (!(radius > 0) || !std::isfinite(radius))
+    return fail(CKD_ERR_BAD_ARG, "Radius must be a positive number");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !q_offsets || (fill ? (!offsets || !idx || !dist) : !counts))
+    return fail(CKD_ERR_BAD_ARG, "null query, offset or output pointer");
+  if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* qroot = nullptr;
+  CKD_CUDA(dev_alloc((void**)&qroot, sizeof(int32_t) * nq, s));
+  ckd_status st = csr_owner(q_offsets, (int32_t)t->n_trees, nq, qroot, s);
+  if (st == CKD_OK)
+    st = ball_run(t, q, nq, radius, fill, sorted, counts, offsets, idx, dist, s, qroot);
+  dev_free(qroot, s);
+  return st;
+}
+
+ckd_status ckd_forest_ball_count(const ckd_tree* t, const double* q, const int64_t* q_offsets,
+                                 int64_t nq, double radius, int64_t* counts, void* stream) {
+  return forest_ball(t, q, q_offsets, nq, radius, false, 0, counts, nullptr, nullptr, nullptr,
+                     stream);
+}
+
+ckd_status ckd_forest_ball_fill(const ckd_tree* t, const double* q, const int64_t* q_offsets,
+                                int64_t nq, double radius, int sorted, const int64_t* offsets,
+                                int64_t* idx, double* dist, void* stream) {
+  return forest_ball(t, q, q_offsets, nq, radius, true, sorted, nullptr, offsets, idx, dist,
+                     stream);
 }
 
 ckd_status ckd_release_cached_memory(void) {

@@ -26,7 +26,7 @@ namespace {
 
 constexpr int kStack = 96;
 
-template <int D, bool PER, bool FILL>
+template <int D, bool PER, bool FILL, bool ROOTS = false>
 __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restrict__ Q,
                                               const int32_t* __restrict__ order, int64_t nq_max,
                                               const unsigned* __restrict__ nq_dev,
@@ -34,11 +34,19 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
                                               int stack_len, int64_t* __restrict__ counts,
                                               const int64_t* __restrict__ offsets,
                                               int64_t* __restrict__ oidx,
-                                              double* __restrict__ odist, int want_d2) {
+                                              double* __restrict__ odist, int want_d2,
+                                              const int32_t* __restrict__ qroot) {
+  // packet stack entries; with ROOTS (forests) each entry also carries the lanes
+  // whose balls reached its parent, and the search starts one entry per distinct
+  // root among the warp's queries
   __shared__ int32_t sstk[4][kStack];
+  __shared__ unsigned smsk[4][ROOTS ? kStack : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int64_t gw = (int64_t)blockIdx.x * nw + w;
-  int32_t* stk = gstack ? gstack + gw * stack_len : sstk[w];
+  int32_t* stk = gstack ? gstack + gw * 2 * stack_len : sstk[w];
+  unsigned* msk = gstack && ROOTS
+                      ? reinterpret_cast<unsigned*>(gstack + gw * 2 * stack_len + stack_len)
+                      : smsk[w];
   const int64_t nq = nq_dev ? (int64_t)*nq_dev : nq_max;
   if (gw * 32 >= nq) return;  // whole warp past the (device-side) query count
   int64_t slot = gw * 32 + lane;
@@ -53,14 +61,28 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
   const int64_t cur_end = (FILL && valid) ? offsets[qi + 1] : 0;
   int32_t cov_lo = 0, cov_hi = 0;  // point range already counted whole (count pass)
   int top = 0;
-  if (lane == 0) stk[0] = 0;
+  if (ROOTS) {
+    const int32_t root = valid ? qroot[qi] : -1;
+    const unsigned grp = __match_any_sync(0xffffffffu, root);
+    const bool leader = valid && lane == __ffs(grp) - 1;
+    const unsigned leaders = __ballot_sync(0xffffffffu, leader);
+    if (leader) {
+      const int e = __popc(leaders & ((1u << lane) - 1u));
+      stk[e] = root;
+      msk[e] = grp;
+    }
+    top = __popc(leaders) - 1;
+  } else if (lane == 0) {
+    stk[0] = 0;
+  }
   __syncwarp();
   while (top >= 0) {
     int32_t node = stk[top];
+    const unsigned em = ROOTS ? msk[top] : 0xffffffffu;
     --top;
     __syncwarp();
     NodeMeta m = load_meta(tv.meta, node);
-    bool need = box_mind2<D, PER>(tv, q, node) <= rr;
+    bool need = ((em >> lane) & 1u) && box_mind2<D, PER>(tv, q, node) <= rr;
     if (!FILL && need && m.start >= cov_lo && m.start < cov_hi) need = false;
     if (!FILL && need && m.left >= 0 &&
         (PER ? box_maxd2_near<D>(tv, q, node) : box_maxd2<D>(tv, q, node)) <= rr) {
@@ -90,6 +112,10 @@ __global__ void __launch_bounds__(128) k_ball(TreeView tv, const double* __restr
       if (lane == 0) {
         stk[top + 1] = m.left + 1;
         stk[top + 2] = m.left;
+        if (ROOTS) {
+          msk[top + 1] = nm;
+          msk[top + 2] = nm;
+        }
       }
       top += 2;
       __syncwarp();
@@ -282,7 +308,8 @@ __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const doubl
                                                         int64_t* __restrict__ oidx,
                                                         double* __restrict__ odist, int want_d2,
                                                         EmitTask* __restrict__ tasks,
-                                                        unsigned* __restrict__ n_tasks) {
+                                                        unsigned* __restrict__ n_tasks,
+                                                        const int32_t* __restrict__ qroot) {
   __shared__ int32_t sstk[4][kHeavyStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -296,7 +323,7 @@ __global__ void __launch_bounds__(128) k_ball_fill_warp(TreeView tv, const doubl
     int64_t cur = offsets[qi];
     const int64_t cur_end = offsets[qi + 1];
     int top = 0;
-    if (lane == 0) stk[0] = 0;
+    if (lane == 0) stk[0] = qroot ? qroot[qi] : 0;
     __syncwarp();
     while (top >= 0) {
       const int32_t node = stk[top];
@@ -741,15 +768,16 @@ __global__ void __launch_bounds__(128) k_box(TreeView tv, const double* __restri
 template <int D, bool PER>
 ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq,
                        double r, bool fill, int sorted, int64_t* counts, const int64_t* offsets,
-                       int64_t* idx, double* dist, cudaStream_t s) {
+                       int64_t* idx, double* dist, cudaStream_t s, const int32_t* qroot) {
   TreeView tv = t->view();
   const int threads = 128, nw = threads / 32;
   int64_t warps = cdiv(nq, 32);
   unsigned blocks = (unsigned)cdiv(warps, nw);
-  int stack_len = std::max(kStack, t->depth + 4);
+  // a packet stack holds at most one pending sibling per level, plus the roots
+  int stack_len = std::max(kStack, t->depth + 4 + (qroot ? 32 : 0));
   int32_t* gstack = nullptr;
   if (stack_len > kStack)
-    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * stack_len * (int64_t)blocks * nw, s));
+    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw, s));
   double r2 = r * r;  // radius**2 (cosmokdtree.f90:1112)
   if (fill) {
     // heavy rows: a warp per query; light rows: the per-lane kernel over a list
@@ -762,9 +790,14 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     k_split_rows<<<(unsigned)cdiv(nq, 256), 256, 0, s>>>(offsets, order, nq, heavy, cnt, light,
                                                          cnt + 1);
     CKD_LAUNCH_CHECK();
-    k_ball<D, PER, true><<<blocks, threads, 0, s>>>(tv, q, light, nq, cnt + 1, r2, gstack,
-                                                     stack_len, nullptr, offsets, idx, dist,
-                                                     sorted ? 1 : 0);
+    if (qroot)
+      k_ball<D, PER, true, true><<<blocks, threads, 0, s>>>(tv, q, light, nq, cnt + 1, r2, gstack,
+                                                            stack_len, nullptr, offsets, idx,
+                                                            dist, sorted ? 1 : 0, qroot);
+    else
+      k_ball<D, PER, true><<<blocks, threads, 0, s>>>(tv, q, light, nq, cnt + 1, r2, gstack,
+                                                       stack_len, nullptr, offsets, idx, dist,
+                                                       sorted ? 1 : 0, nullptr);
     CKD_LAUNCH_CHECK();
     int dev = 0, sms = 148;
     CKD_CUDA(cudaGetDevice(&dev));
@@ -780,7 +813,7 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     CKD_CUDA(cudaMemsetAsync(ntask, 0, sizeof(unsigned), s));
     k_ball_fill_warp<D, PER><<<(unsigned)std::max<int64_t>(1, hblocks), 128, 0, s>>>(
         tv, q, heavy, cnt, r2, hstack, hstack_len, offsets, idx, dist, sorted ? 1 : 0, tasks,
-        ntask);
+        ntask, qroot);
     CKD_LAUNCH_CHECK();
     k_ball_emit<D, PER><<<(unsigned)sms * 8, 128, 0, s>>>(tv, q, tasks, ntask, idx, dist,
                                                           sorted ? 1 : 0);
@@ -789,9 +822,14 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
                     (void*)ntask})
       dev_free(p, s);
   } else {
-    k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2, gstack,
-                                                      stack_len, counts, nullptr, nullptr, nullptr,
-                                                      0);
+    if (qroot)
+      k_ball<D, PER, false, true><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2,
+                                                             gstack, stack_len, counts, nullptr,
+                                                             nullptr, nullptr, 0, qroot);
+    else
+      k_ball<D, PER, false><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2, gstack,
+                                                        stack_len, counts, nullptr, nullptr,
+                                                        nullptr, 0, nullptr);
     CKD_LAUNCH_CHECK();
   }
   if (fill && sorted) {
@@ -874,22 +912,24 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
 }  // namespace
 
 bool want_order(const ckd_tree* t, int64_t nq);
+ckd_status query_order_roots(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
+                             const int32_t* qroot, cudaStream_t s);
 
 ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bool fill, int sorted,
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
-                    cudaStream_t s) {
+                    cudaStream_t s, const int32_t* qroot) {
   int32_t* order = nullptr;
   if (want_order(t, nq)) {
     CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
-    CKD_TRY(query_order(t, q, nq, order, s));
+    CKD_TRY(query_order_roots(t, q, nq, order, qroot, s));
   }
   ckd_status st;
 #define CKD_BALL_CASE(DD)                                                                      \
   case DD:                                                                                     \
     st = t->periodic ? ball_launch<DD, true>(t, q, order, nq, r, fill, sorted, counts, offsets, \
-                                             idx, dist, s)                                     \
+                                             idx, dist, s, qroot)                              \
                      : ball_launch<DD, false>(t, q, order, nq, r, fill, sorted, counts,         \
-                                              offsets, idx, dist, s);                          \
+                                              offsets, idx, dist, s, qroot);                   \
     break;
   switch (t->d) {
     CKD_BALL_CASE(1)

@@ -2784,6 +2784,18 @@ ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* 
   return query_order(t, q, nq, order, nullptr, s);
 }
 
+// leaf order of queries that each start at their own tree's root (forests)
+ckd_status query_order_roots(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
+                             const int32_t* qroot, cudaStream_t s) {
+  switch (t->d) {
+#define CKD_QO(DD) \
+  case DD: return order_impl<DD>(t, q, nq, order, nullptr, s, nullptr, qroot);
+    CKD_QO(1) CKD_QO(2) CKD_QO(3) CKD_QO(4) CKD_QO(5) CKD_QO(6) CKD_QO(7) CKD_QO(8)
+#undef CKD_QO
+  }
+  return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
+}
+
 // Queries are ordered by leaf when there are enough of them to fill many warps.
 // (tuning key 6: 0 automatic, 1 always, 2 never)
 bool want_order(const ckd_tree* t, int64_t nq) {

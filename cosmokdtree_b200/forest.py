@@ -140,6 +140,32 @@ class Forest:
                                             _ptr(idx), _stream()))
         return offsets, idx
 
+    def ball_csr(self, queries, query_offsets, radius, sorted=False):
+        """Points within ``radius`` of each query (rows grouped by tree like the kNN
+        queries), as CSR CUDA tensors (offsets (nq+1,), idx local to the query's
+        tree, dist); ``sorted`` orders each row by (distance, id)."""
+        radius = float(radius)
+        if not radius > 0:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "Radius must be a positive number")
+        L = _lib.load()
+        with torch.cuda.device(self.device):
+            q, qo = self._grouped(queries, query_offsets, "queries", self.d)
+            nq = q.shape[0]
+            counts = torch.empty(nq, dtype=torch.int64, device=q.device)
+            offsets = torch.zeros(nq + 1, dtype=torch.int64, device=q.device)
+            if nq > 0:
+                check(L.ckd_forest_ball_count(self.handle, _ptr(q), _ptr(qo), nq, radius,
+                                              _ptr(counts), _stream()))
+                check(L.ckd_exclusive_scan(_ptr(counts), _ptr(offsets), nq, _stream()))
+            total = int(offsets[-1].item())
+            idx = torch.empty(total, dtype=torch.int64, device=q.device)
+            dist = torch.empty(total, dtype=torch.float64, device=q.device)
+            if nq > 0 and total > 0:
+                check(L.ckd_forest_ball_fill(self.handle, _ptr(q), _ptr(qo), nq, radius,
+                                             int(bool(sorted)), _ptr(offsets), _ptr(idx),
+                                             _ptr(dist), _stream()))
+        return offsets, idx, dist
+
 
 def build_forest(points, offsets=None, leaf=16, boxsize=None) -> Forest:
     """Build every tree of a forest in one pass.  ``points`` is an (N, d) array

@@ -233,6 +233,15 @@ ckd_status ckd_forest_box_count(const ckd_tree* forest, const double* boxes_dev,
 ckd_status ckd_forest_box_fill(const ckd_tree* forest, const double* boxes_dev,
                                const int64_t* b_offsets_dev, int64_t nb,
                                const int64_t* offsets_dev, int64_t* idx_dev, void* stream);
+/* Ball search over a forest, queries grouped by tree as for ckd_forest_knn;
+ * two-phase CSR as ckd_ball_* (ids local to each query's tree). */
+ckd_status ckd_forest_ball_count(const ckd_tree* forest, const double* q_dev,
+                                 const int64_t* q_offsets_dev, int64_t nq, double radius,
+                                 int64_t* counts_dev, void* stream);
+ckd_status ckd_forest_ball_fill(const ckd_tree* forest, const double* q_dev,
+                                const int64_t* q_offsets_dev, int64_t nq, double radius,
+                                int sorted, const int64_t* offsets_dev, int64_t* idx_dev,
+                                double* dist_dev, void* stream);
 
 /* Save a built tree or forest to a file / load it onto the current device (no
  * counterpart in the reference, which rebuilds on every run).  The file is a raw

@@ -84,6 +84,41 @@ def test_forest_box_matches_single_trees(gpu):
             np.testing.assert_array_equal(np.sort(a), np.nonzero(m)[0])
 
 
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("sorted_", [False, True])
+def test_forest_ball_matches_single_trees(gpu, oracle, periodic, sorted_):
+    """Forest ball search: each tree's rows equal the single-tree search of the same
+    points (same order), and the oracle's on a few trees.  Enough queries to take
+    the leaf-ordered path, warps spanning several trees, and rows past 256 results
+    (the warp-per-row fill)."""
+    from cosmokdtree_b200 import kdtree, build_forest
+    rng = np.random.default_rng(64 + periodic)
+    pts = _forest_points(44, 64 + periodic, periodic)
+    box = 1.0 if periodic else None
+    f = build_forest(pts, leaf=16, boxsize=box)
+    qs = _queries_per_tree(pts, rng, 0.3)
+    qoff = np.concatenate([[0], np.cumsum([len(q) for q in qs])])
+    r = 0.06
+    off, idx, dist = (x.cpu().numpy() for x in f.ball_csr(qs, qoff, r, sorted=sorted_))
+    assert np.diff(off).max() >= 256
+    for t, (P, Q) in enumerate(zip(pts, qs)):
+        tr = kdtree.build_kdtree(P, leaf=16, boxsize=box)
+        o1, i1, d1 = (x.cpu().numpy() for x in kdtree.ball_search_csr(tr, Q, r, sorted=sorted_))
+        rows = slice(qoff[t], qoff[t + 1] + 1)
+        np.testing.assert_array_equal(off[rows] - off[qoff[t]], o1)
+        lo, hi = off[qoff[t]], off[qoff[t + 1]]
+        np.testing.assert_array_equal(idx[lo:hi], i1)
+        np.testing.assert_array_equal(dist[lo:hi], d1)
+        if t % 11 == 3:
+            ot = oracle.OracleTree(P, 16, [1.0] * 3 if periodic else None)
+            oo, oi, od = ot.ball_csr(Q, r, sorted=sorted_)
+            np.testing.assert_array_equal(o1, oo)
+            if sorted_ or not periodic:
+                np.testing.assert_array_equal(i1, oi)
+                np.testing.assert_array_equal(d1, od)
+    f.close()
+
+
 def test_forest_knn_cuda_graph(gpu):
     import torch
     from cosmokdtree_b200 import build_forest
