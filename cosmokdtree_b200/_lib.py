@@ -79,6 +79,7 @@ SIGNATURES = {
     "ckd_tree_export": [_vp, _pi32, _pdbl, _pi64, _pi64, _pi64, _pi64, _pdbl, _pdbl, _pi64],
     "ckd_knn": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
     "ckd_knn_host": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
+    "ckd_knn_multi_k": [_vp, _vp, _i64, _vp, _int, _int, _vp, _vp, _vp],
     "ckd_knn_noalloc": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],
     "ckd_query_order": [_vp, _vp, _i64, _vp, _vp],
     "ckd_knn_ordered": [_vp, _vp, _i64, _vp, _int, _int, _vp, _vp, _vp],

@@ -107,6 +107,8 @@ cudaError_t dev_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) :
 ckd_status build_dispatch(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t s);
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s);
+ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* kq,
+                       int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s);
 ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
                        int sorted, double* dist, int64_t* idx, cudaStream_t s);
 ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
@@ -434,6 +436,17 @@ ckd_status ckd_knn(const ckd_tree* t, const double* q, int64_t nq, int k, int so
   if (nq == 0) return CKD_OK;
   if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
   return knn_run(t, q, nq, k, sorted, dist, idx, (cudaStream_t)stream);
+}
+
+ckd_status ckd_knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* k_dev,
+                           int kmax, int sorted, double* dist, int64_t* idx, void* stream) {
+  CKD_TRY(check_single(t));
+  if (kmax < 1 || kmax > 65536) return fail(CKD_ERR_BAD_ARG, "kmax must be 1..65536");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (nq == 0) return CKD_OK;
+  if (!q || !k_dev || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query, k or output pointer");
+  if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
+  return knn_multi_k(t, q, nq, k_dev, kmax, sorted, dist, idx, (cudaStream_t)stream);
 }
 
 ckd_status ckd_query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,

@@ -33,7 +33,7 @@ from ._lib import CKDArgumentError, check
 
 __all__ = [
     "KDTree", "build_kdtree", "deallocate_kdtree", "knn_search", "ball_search", "box_search",
-    "knn_search_batch", "ball_search_csr", "box_search_csr", "box_search_periodic_csr",
+    "knn_search_batch", "knn_search_multi_k", "ball_search_csr", "box_search_csr", "box_search_periodic_csr",
     "save_kdtree", "load_kdtree", "read_fortran_points", "release_cached_memory",
 ]
 
@@ -232,6 +232,34 @@ def knn_search(tree: KDTree, target, k, sorted=True):
     if _on_device(target):
         return dist, idx
     with torch.cuda.device(tree.device):
+        return _to_host(dist), _to_host(idx)
+
+
+def knn_search_multi_k(tree: KDTree, target, ks, sorted=True):
+    """k nearest neighbours with a k per target point, in one call.  ``ks`` holds
+    one positive integer per target row.  Returns (dist, idx) of shape
+    (ntar, max(ks)); a row's slots past its own k hold id -2 and distance
+    1.8446743523953730e19 (the k > n marker).  numpy for host input, CUDA tensors
+    for CUDA-tensor input."""
+    with torch.cuda.device(tree.device):
+        q, _ = _queries(tree, target)
+        nq = q.shape[0]
+        kt = torch.as_tensor(np.asarray(ks) if not isinstance(ks, torch.Tensor) else ks)
+        if kt.dim() != 1 or kt.shape[0] != nq:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "ks must hold one k per target row")
+        if kt.dtype.is_floating_point or kt.dtype == torch.bool:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be an integer")
+        kt = kt.to(device=q.device, dtype=torch.int32).contiguous()
+        kmax = int(kt.max().item()) if nq > 0 else 1
+        if nq > 0 and int(kt.min().item()) < 1:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be a positive integer")
+        dist = torch.empty((nq, kmax), dtype=torch.float64, device=q.device)
+        idx = torch.empty((nq, kmax), dtype=torch.int64, device=q.device)
+        if nq > 0:
+            check(_lib.load().ckd_knn_multi_k(tree.handle, _ptr(q), nq, _ptr(kt), kmax,
+                                              int(bool(sorted)), _ptr(dist), _ptr(idx), _stream()))
+        if _on_device(target):
+            return dist, idx
         return _to_host(dist), _to_host(idx)
 
 

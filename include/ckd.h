@@ -160,6 +160,16 @@ ckd_status ckd_kernel_ms(float* ms);
 ckd_status ckd_knn_noalloc(const ckd_tree* tree, const double* q_dev, int64_t nq, int k,
                            int sorted, double* dist_dev, int64_t* idx_dev, void* stream);
 
+/* kNN with a k per query in one call (k_dev[nq], each in 1..kmax; no reference
+ * counterpart: the reference takes one k per call, src/cosmokdtree.f90:504-540).
+ * Outputs are (nq, kmax) row-major; slots past a query's own k hold id -2 and
+ * distance sqrt(HUGE(0.0)) = 1.8446743523953730e19, the k > n marker.  Queries
+ * are grouped by k on the device and each group takes the ckd_knn path, so rows
+ * equal ckd_knn's for their k.  Reads the k histogram back (synchronises). */
+ckd_status ckd_knn_multi_k(const ckd_tree* tree, const double* q_dev, int64_t nq,
+                           const int32_t* k_dev, int kmax, int sorted, double* dist_dev,
+                           int64_t* idx_dev, void* stream);
+
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);

@@ -416,3 +416,30 @@ def test_gpu_host_csr_entry_points(gpu, oracle):
     empty = np.zeros(1, np.int64)
     _lib.check(L.ckd_box_count_host(t.handle, vp(B), 0, vp(empty), None))
     assert empty[0] == 0
+
+
+def test_gpu_knn_multi_k(gpu, oracle):
+    """One call with a k per query: each row equals the single-k search (and the
+    oracle) for its k, padded past its k with the missing-neighbour marker."""
+    import torch
+    P = make_points("clustered", 40000, 3, True, seed=7)
+    rng = np.random.default_rng(31)
+    Q = np.concatenate([P[rng.integers(0, len(P), 6000)], rng.random((3000, 3)) - 0.5])
+    ks = rng.choice([1, 5, 8, 32, 64, 100], len(Q))
+    t = gpu.kdtree.build_kdtree(P, boxsize=1.0)
+    d, i = gpu.kdtree.knn_search_multi_k(t, Q, ks)
+    assert d.shape == (len(Q), 100) and i.shape == (len(Q), 100)
+    ot = oracle.OracleTree(P, 16, 1.0)
+    for k in np.unique(ks):
+        rows = np.nonzero(ks == k)[0]
+        d1, i1 = gpu.kdtree.knn_search(t, Q[rows], int(k))
+        np.testing.assert_array_equal(i[rows, :k], i1)
+        np.testing.assert_array_equal(d[rows, :k], d1)
+        assert (i[rows, k:] == -2).all() and (d[rows, k:] == 1.8446743523953730e19).all()
+        od, oi = ot.knn(Q[rows[:200]], int(k))
+        np.testing.assert_array_equal(i1[:200], oi)
+    dt, it = gpu.kdtree.knn_search_multi_k(t, torch.from_numpy(Q).cuda(),
+                                           torch.from_numpy(ks).cuda(), sorted=False)
+    np.testing.assert_array_equal(np.sort(it.cpu().numpy(), 1), np.sort(i, 1))
+    with pytest.raises(AssertionError):
+        gpu.kdtree.knn_search_multi_k(t, Q[:3], [1, 0, 2])
