@@ -399,6 +399,11 @@ __device__ __forceinline__ int32_t tile_chunk_prefix(const unsigned (&msk)[kItem
 // midpoint splits (x < split goes left, cosmokdtree.f90:470).  A sliding split
 // sends exactly one point, the first holding the extreme (:376-403), to the
 // side that would be empty; its positions count 0 here and record that point.
+// Each thread takes 8 consecutive positions (vector loads of the node ids and,
+// when they all belong to one node, of that node's split coordinate), so the
+// chain node id -> split record -> coordinate costs three loads per thread
+// instead of three per position.  The left flags go to a bitmap (bit p & 31 of
+// word p >> 5) that the scatter reads back.
 __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ NID,
                                                const FlagRec* __restrict__ frec,
@@ -407,40 +412,72 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                int32_t* __restrict__ pstart,
                                                int32_t* __restrict__ pend,
                                                unsigned* __restrict__ flags) {
-  constexpr int W = kBT / 32;
-  __shared__ int32_t cpre[kItems * W + 1];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-  unsigned msk[kItems];
-  int32_t av[kItems];
-  unsigned se = 0;  // bit 2 it: segment start, bit 2 it + 1: segment end
+  static_assert(kItems == 8, "8 consecutive positions per thread");
+  __shared__ int32_t tmp[kBT / 32];
+  const int lane = threadIdx.x & 31;
+  const int64_t p0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
+  int32_t a[kItems];
+  const bool full = p0 + kItems <= nw;
+  const bool vec = full && (n & 1) == 0 && (reinterpret_cast<uintptr_t>(NID) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  if (vec) {
+    const int4 u = __ldg(reinterpret_cast<const int4*>(NID + p0));
+    const int4 v = __ldg(reinterpret_cast<const int4*>(NID + p0) + 1);
+    a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w, a[4] = v.x, a[5] = v.y, a[6] = v.z, a[7] = v.w;
+  } else {
 #pragma unroll
-  for (int it = 0; it < kItems; ++it) {
-    const int64_t p = base + (int64_t)it * kBT + threadIdx.x;
-    const int32_t a = p < nw ? NID[p] : -1;
-    int f = 0;
-    if (a >= 0) {
-      const FlagRec r = frec[a];
-      const double x = X[(int64_t)r.axis * n + p];
-      if (r.md == 0) f = x < r.split ? 1 : 0;
-      else if (x == r.split) atomicMin(&ext[a], (int32_t)p);
-      if (p == r.wst) se |= 1u << (2 * it);
-      if (p == (int64_t)r.wst + r.count - 1) se |= 2u << (2 * it);
+    for (int i = 0; i < kItems; ++i) a[i] = p0 + i < nw ? NID[p0 + i] : -1;
+  }
+  bool single = a[0] >= 0;
+#pragma unroll
+  for (int i = 1; i < kItems; ++i) single = single && a[i] == a[0];
+  unsigned f8 = 0, se = 0;  // left flags; segment start (bit 2i) and end (bit 2i+1)
+  auto one = [&](int i, const FlagRec& r, double x) {
+    const int64_t p = p0 + i;
+    if (r.md == 0) f8 |= (x < r.split ? 1u : 0u) << i;
+    else if (x == r.split) atomicMin(&ext[a[i]], (int32_t)p);
+    if (p == r.wst) se |= 1u << (2 * i);
+    if (p == (int64_t)r.wst + r.count - 1) se |= 2u << (2 * i);
+  };
+  if (single && vec) {
+    const FlagRec r = frec[a[0]];
+    const double2* xr = reinterpret_cast<const double2*>(X + (int64_t)r.axis * n + p0);
+#pragma unroll
+    for (int h = 0; h < kItems / 2; ++h) {
+      const double2 x = __ldg(xr + h);
+      one(2 * h, r, x.x);
+      one(2 * h + 1, r, x.y);
     }
-    msk[it] = __ballot_sync(0xffffffffu, f);
-    av[it] = a;
-    if (lane == 0) flags[(base >> 5) + it * W + w] = msk[it];
-  }
-  const int32_t tot = tile_chunk_prefix(msk, cpre);
-  const unsigned lt = (1u << lane) - 1u;
+  } else {
+    FlagRec r;
+    int32_t ra = -1;
 #pragma unroll
-  for (int it = 0; it < kItems; ++it) {
-    const unsigned b = (se >> (2 * it)) & 3u;
-    if (b == 0) continue;
-    const int32_t ex = cpre[it * W + w] + __popc(msk[it] & lt);
-    if (b & 1u) pstart[av[it]] = ex;
-    if (b & 2u) pend[av[it]] = ex + (int32_t)((msk[it] >> lane) & 1u);
+    for (int i = 0; i < kItems; ++i) {
+      if (a[i] < 0) continue;
+      if (a[i] != ra) {
+        r = frec[a[i]];
+        ra = a[i];
+      }
+      one(i, r, X[(int64_t)r.axis * n + p0 + i]);
+    }
   }
+  int32_t tot;
+  const int32_t ex = block_exclusive_scan<int32_t, kBT>(__popc(f8), tmp, tot);
+  if (se) {
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      const unsigned b = (se >> (2 * i)) & 3u;
+      if (b == 0) continue;
+      const int32_t e = ex + __popc(f8 & ((1u << i) - 1u));
+      if (b & 1u) pstart[a[i]] = e;
+      if (b & 2u) pend[a[i]] = e + (int32_t)((f8 >> i) & 1u);
+    }
+  }
+  // 4 lanes (32 positions) per bitmap word
+  unsigned word = f8 << (8 * (lane & 3));
+  word |= __shfl_xor_sync(0xffffffffu, word, 1);
+  word |= __shfl_xor_sync(0xffffffffu, word, 2);
+  if ((lane & 3) == 0) flags[p0 >> 5] = word;
   if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
 }
 
