@@ -678,6 +678,17 @@ def main():
         if it < n_builds - 1:
             tree.close()
     build_ms_v = allmax(float(np.mean(build_ms)))
+    # the input's host-to-device copy (pinned host buffer), reported beside the build
+    P_pin = torch.from_numpy(P).pin_memory()
+    Pd2 = torch.empty_like(Pd)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    Pd2.copy_(P_pin, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    build_h2d_ms = allmax(e0.elapsed_time(e1))
+    del P_pin, Pd2
 
     # ---- kNN, inputs resident in HBM
     nq = P.shape[0]
@@ -922,6 +933,7 @@ def main():
                                          "gpu_launches": int(ball_launches)},
                      "count_parity_sample": ball_parity},
             "build": {"ms": build_ms_v, "mpts_per_s": n / (build_ms_v / 1e3) / 1e6,
+                      "input_h2d_ms": build_h2d_ms,
                       "cpu_s": cpu_build_s, "cpu_mpts_per_s": n / cpu_build_s / 1e6,
                       "n_nodes": tree.n_nodes, "depth": tree.depth},
             "breakdown_ms": {"learned_step": float(np.mean(learned_steps)),
