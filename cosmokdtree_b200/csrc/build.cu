@@ -578,9 +578,36 @@ __global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMe
   srec[2 * (int64_t)a + 1] = make_int4(md == 0 ? pbase[a] : ext[a], c0, wl, wr);
 }
 
+// bulk asynchronous copies (global -> this CTA's shared memory) completing on an
+// mbarrier; every wait is bounded
+constexpr unsigned kBarWaitLimit = 1u << 24;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ bool bar_wait0(uint32_t bar) {
+  for (unsigned it = 0; it < kBarWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(done) : "r"(bar), "r"(0u) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// scatter tile staging: dynamic shared memory of the staged scatter
+__host__ __device__ constexpr size_t scatter_smem(int d) {
+  return (size_t)d * kTile * sizeof(double) + (size_t)kTile * sizeof(int32_t);
+}
+
 // Stable partition of every open segment: points of open children go to the
 // next working set, points of new leaves to the final leaf-ordered arrays.
-template <int D>
+// STAGED: the tile's coordinate rows and ids are brought into shared memory by
+// bulk asynchronous copies issued at the start (one per row, 16-byte aligned
+// because the working rows have an even stride), overlapping the first pass and
+// the tile scan; the second pass then reads them from shared memory.
+template <int D, bool STAGED>
 __global__ void __launch_bounds__(kBT) k_scatter(
     const double* __restrict__ X, const int32_t* __restrict__ I, const int32_t* __restrict__ NID,
     const int4* __restrict__ srec, const int32_t* __restrict__ tile_off,
@@ -589,8 +616,38 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     int32_t* __restrict__ If, int32_t* __restrict__ err) {
   constexpr int W = kBT / 32;
   __shared__ int32_t cpre[kItems * W + 1];
+  __shared__ __align__(8) unsigned long long bar;
+  extern __shared__ __align__(16) unsigned char stage[];
+  double* sx = reinterpret_cast<double*>(stage);
+  int32_t* si = reinterpret_cast<int32_t*>(stage + (size_t)D * kTile * sizeof(double));
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTile;
+  if (STAGED) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int64_t cnt = min((int64_t)kTile, nw - base);
+      const uint32_t bx = (uint32_t)(((cnt + 1) & ~1ll) * 8), bi = (uint32_t)(((cnt + 3) & ~3ll) * 4);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&bar)),
+                   "r"(D * bx + bi)
+                   : "memory");
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(smem_u32(sx + j * kTile)),
+            "l"(X + (int64_t)j * n + base), "r"(bx), "r"(smem_u32(&bar))
+            : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(smem_u32(si)),
+          "l"(I + base), "r"(bi), "r"(smem_u32(&bar))
+          : "memory");
+    }
+  }
   unsigned msk[kItems];
   int32_t av[kItems];
 #pragma unroll
@@ -600,6 +657,11 @@ __global__ void __launch_bounds__(kBT) k_scatter(
     msk[it] = flags[(base >> 5) + it * W + w];  // the flag pass's ballot of these 32 positions
   }
   tile_chunk_prefix(msk, cpre);
+  if (STAGED && !bar_wait0(smem_u32(&bar))) {
+    atomicExch(err, 3);             // copies did not land: report, let them finish, leave
+    bar_wait0(smem_u32(&bar));
+    return;
+  }
   const int32_t run = tile_off[blockIdx.x];
   const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
@@ -627,17 +689,21 @@ __global__ void __launch_bounds__(kBT) k_scatter(
       atomicExch(err, 2);
       continue;
     }
-    const int32_t id = I[p];
+    const int t = (int)(p - base);
+    const int32_t id = STAGED ? si[t] : I[p];
+    double xv[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) xv[j] = STAGED ? sx[j * kTile + t] : X[(int64_t)j * n + p];
     const int32_t wc = f ? r1.z : r1.w;  // child's working start, negative for a leaf
     if (wc < 0) {
       const int64_t dst = (int64_t)start + (f ? 0 : nl) + rank;
 #pragma unroll
-      for (int j = 0; j < D; ++j) Pf[(int64_t)j * n + dst] = X[(int64_t)j * n + p];
+      for (int j = 0; j < D; ++j) Pf[(int64_t)j * n + dst] = xv[j];
       If[dst] = id;
     } else {
       const int64_t wd = (int64_t)wc + rank;
 #pragma unroll
-      for (int j = 0; j < D; ++j) Xo[(int64_t)j * n + wd] = X[(int64_t)j * n + p];
+      for (int j = 0; j < D; ++j) Xo[(int64_t)j * n + wd] = xv[j];
       Io[wd] = id;
       NIDo[wd] = r1.y + (f ? 0 : 1);
     }
@@ -857,7 +923,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   const int64_t ntiles = cdiv(n, kTile);
   for (int b = 0; b < 2; ++b) {
     CKD_CUDA(dev_alloc((void**)&B.X[b], sizeof(double) * D * n, s));
-    CKD_CUDA(dev_alloc((void**)&B.I[b], sizeof(int32_t) * n, s));
+    CKD_CUDA(dev_alloc((void**)&B.I[b], sizeof(int32_t) * (n + 4), s));  // + the copy's rounding
     CKD_CUDA(dev_alloc((void**)&B.NID[b], sizeof(int32_t) * n, s));
   }
   int64_t max_open = n / (leaf + 1) + 2 + t->n_trees;
@@ -969,6 +1035,12 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(cudaStreamSynchronize(s));  // `roots`, `wst0` and `rk` are host buffers of the copies
   dev_free(off_dev, s);
 
+  // the staged scatter needs 16-byte aligned rows (even stride) and fits D <= 4
+  // (<= 72 KB of shared memory per block)
+  const bool staged = D <= 4 && (n & 1) == 0;
+  if (staged)
+    CKD_CUDA(cudaFuncSetAttribute(k_scatter<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)scatter_smem(D)));
   // pinned word for the per-level readback of (next open count, next working size)
   static thread_local int64_t* level_tot = nullptr;
   if (!level_tot) CKD_CUDA(cudaMallocHost((void**)&level_tot, sizeof(int64_t)));
@@ -1004,9 +1076,14 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.mode, B.ext, B.nleft, B.pbase,
                                    B.act[1 - alist], B.wst, B.srec);
     CKD_LAUNCH_CHECK();
-    k_scatter<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off, B.flags,
-                                     n, nw, B.X[1 - cur], B.I[1 - cur], B.NID[1 - cur], t->pts,
-                                     t->ids, B.scal + 1);
+    if (staged)
+      k_scatter<D, true><<<ntw, kBT, scatter_smem(D), s>>>(
+          B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off, B.flags, n, nw, B.X[1 - cur],
+          B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
+    else
+      k_scatter<D, false><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off,
+                                              B.flags, n, nw, B.X[1 - cur], B.I[1 - cur],
+                                              B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
     CKD_LAUNCH_CHECK();
     CKD_CUDA(cudaMemcpyAsync(level_tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
@@ -1060,6 +1137,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
       t->meta, n_nodes, t->box, t->cell, t->pair, t->cell32, t->centre);
   CKD_LAUNCH_CHECK();
   CKD_CUDA(cudaStreamSynchronize(s));
+  if (err == 3) return fail(CKD_ERR_TIMEOUT, "build: a tile copy into shared memory timed out");
   if (err) return fail(CKD_ERR_CUDA, "internal error: inconsistent partition in build");
   // leaves = (nodes + 1) / 2 for each full binary tree
   t->n_leaves = (n_nodes + T) / 2;
