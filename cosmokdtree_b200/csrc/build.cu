@@ -81,6 +81,9 @@ struct BuildBufs {
   int32_t* tile_off = nullptr;
   unsigned* flags = nullptr;  // left flags of the working positions, one bit each
   int32_t* scal = nullptr;  // device scalars: [0] next open count, [1] error flag
+  // level state {open nodes, working points, nodes so far, levels with open nodes},
+  // double-buffered: a level reads lst[p] and its last node kernel writes lst[1-p]
+  int4* lst = nullptr;
 };
 
 // ------------------------------------------------------------------ kernels
@@ -140,10 +143,13 @@ template <int D>
 __global__ void __launch_bounds__(kBT, 5) k_seg_box(const double* __restrict__ X,
                                                  const int32_t* __restrict__ NID,
                                                  int64_t n, int64_t nw,
-                                                 unsigned long long* __restrict__ keys) {
+                                                 unsigned long long* __restrict__ keys,
+                                                 const int4* __restrict__ st = nullptr) {
   constexpr int W = kBT / 32;
   __shared__ int32_t rec_id[W][2];
   __shared__ unsigned long long rec_v[W][2][2 * D];
+  if (st) nw = st->y;  // working points of this level (device state)
+  if ((int64_t)blockIdx.x * kTile >= nw) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t p0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
   // node of every position (-1 past the working set), run breaks inside the thread
@@ -305,13 +311,14 @@ __global__ void __launch_bounds__(kBT, 5) k_seg_box(const double* __restrict__ X
 
 // Split decision per open node (cosmokdtree.f90:347-410).
 template <int D>
-__global__ void k_decide(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
+__global__ void k_decide(const int32_t* __restrict__ act, const int4* __restrict__ st,
+                         NodeMeta* __restrict__ meta,
                          double* __restrict__ cell, double* __restrict__ box,
                          const unsigned long long* __restrict__ keys, int32_t* __restrict__ mode,
                          int32_t* __restrict__ ext, const int32_t* __restrict__ wst,
                          FlagRec* __restrict__ frec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+  if (i >= st->x) return;
   int32_t a = act[i];
   double lo[D], hi[D], clo[D], chi[D];
 #pragma unroll
@@ -408,12 +415,18 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
                                                const int32_t* __restrict__ NID,
                                                const FlagRec* __restrict__ frec,
                                                int32_t* __restrict__ ext, int64_t n,
-                                               int64_t nw, int32_t* __restrict__ tile_sum,
+                                               const int4* __restrict__ st,
+                                               int32_t* __restrict__ tile_sum,
                                                int32_t* __restrict__ pstart,
                                                int32_t* __restrict__ pend,
                                                unsigned* __restrict__ flags) {
   static_assert(kItems == 8, "8 consecutive positions per thread");
   __shared__ int32_t tmp[kBT / 32];
+  const int64_t nw = st->y;
+  if ((int64_t)blockIdx.x * kTile >= nw) {  // past this level's working set
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = 0;
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int64_t p0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
   int32_t a[kItems];
@@ -484,16 +497,21 @@ __global__ void __launch_bounds__(kBT) k_flags(const double* __restrict__ X,
 // n_left, child pairs and cells; counts the next open list and its working
 // points (cosmokdtree.f90:412-448)
 template <int D>
-__global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __restrict__ meta,
+__global__ void k_children(const int32_t* __restrict__ act, const int4* __restrict__ st, int mb,
+                           NodeMeta* __restrict__ meta,
                            double* __restrict__ cell, const int32_t* __restrict__ pstart,
                            const int32_t* __restrict__ pend, const int32_t* __restrict__ tile_off,
                            const int32_t* __restrict__ wst, const int32_t* __restrict__ mode,
                            const int32_t* __restrict__ ext, int32_t* __restrict__ nleft,
                            int32_t* __restrict__ pbase, unsigned long long* __restrict__ keys,
-                           int32_t first_child, int leaf, int64_t* __restrict__ nxt_cnt,
-                           int32_t* __restrict__ err) {
+                           int leaf, int64_t* __restrict__ nxt_cnt, int32_t* __restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+  const int m = st->x;
+  const int32_t first_child = st->z;
+  if (i >= m) {  // zeros up to the launch bound, so the scan over mb entries is exact
+    if (i < mb) nxt_cnt[i] = 0;
+    return;
+  }
   int32_t a = act[i];
   NodeMeta pm = meta[a];
   const int md = mode[a];
@@ -548,13 +566,22 @@ __global__ void k_children(const int32_t* __restrict__ act, int m, NodeMeta* __r
 }
 
 // next open list (children in list order, so in leaf order) and their working starts
-__global__ void k_next_list(const int32_t* __restrict__ act, int m, const NodeMeta* __restrict__ meta,
+__global__ void k_next_list(const int32_t* __restrict__ act, const int4* __restrict__ st,
+                            int4* __restrict__ st_next, int mb,
+                            const NodeMeta* __restrict__ meta,
                             const int64_t* __restrict__ nxt_off, int leaf,
                             const int32_t* __restrict__ mode, const int32_t* __restrict__ ext,
                             const int32_t* __restrict__ nleft, const int32_t* __restrict__ pbase,
                             int32_t* __restrict__ nxt, int32_t* __restrict__ wst,
                             int4* __restrict__ srec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int4 cs = *st;
+  const int m = cs.x;
+  if (i == 0) {  // the next level's state
+    const int64_t tot = nxt_off[mb];
+    *st_next = make_int4((int32_t)(tot >> 32), (int32_t)(tot & 0xffffffffll), cs.z + 2 * m,
+                         cs.w + (m > 0 ? 1 : 0));
+  }
   if (i >= m) return;
   const int32_t a = act[i];
   const NodeMeta pm = meta[a];
@@ -611,7 +638,8 @@ template <int D, bool STAGED>
 __global__ void __launch_bounds__(kBT) k_scatter(
     const double* __restrict__ X, const int32_t* __restrict__ I, const int32_t* __restrict__ NID,
     const int4* __restrict__ srec, const int32_t* __restrict__ tile_off,
-    const unsigned* __restrict__ flags, int64_t n, int64_t nw, double* __restrict__ Xo,
+    const unsigned* __restrict__ flags, int64_t n, const int4* __restrict__ st,
+    double* __restrict__ Xo,
     int32_t* __restrict__ Io, int32_t* __restrict__ NIDo, double* __restrict__ Pf,
     int32_t* __restrict__ If, int32_t* __restrict__ err) {
   constexpr int W = kBT / 32;
@@ -622,6 +650,8 @@ __global__ void __launch_bounds__(kBT) k_scatter(
   int32_t* si = reinterpret_cast<int32_t*>(stage + (size_t)D * kTile * sizeof(double));
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTile;
+  const int64_t nw = st->y;
+  if (base >= nw) return;  // past this level's working set (the whole block)
   if (STAGED) {
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
@@ -901,7 +931,7 @@ void free_bufs(BuildBufs& B, cudaStream_t s) {
   void* ps[] = {B.X[0],   B.X[1],    B.I[0],      B.I[1],     B.NID[0],  B.NID[1], B.meta,
                 B.cell,   B.box,     B.keys,      B.ext,      B.mode,    B.pstart, B.pend,
                 B.nleft,  B.pbase,   B.wst,       B.act[0],   B.act[1],  B.nxt_cnt, B.nxt_off,
-                B.tile_sum, B.tile_off, B.scal, B.flags, B.frec, B.srec};
+                B.tile_sum, B.tile_off, B.scal, B.flags, B.frec, B.srec, B.lst};
   for (void* p : ps)
     if (p) dev_free(p, s);
   B = BuildBufs();
@@ -934,6 +964,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(dev_alloc((void**)&B.tile_off, sizeof(int32_t) * (ntiles + 1), s));
   CKD_CUDA(dev_alloc((void**)&B.flags, sizeof(unsigned) * ntiles * (kTile / 32), s));
   CKD_CUDA(dev_alloc((void**)&B.scal, sizeof(int32_t) * 4, s));
+  CKD_CUDA(dev_alloc((void**)&B.lst, sizeof(int4) * 2, s));
   CKD_CUDA(cudaMemsetAsync(B.scal, 0, sizeof(int32_t) * 4, s));
 
   // final outputs
@@ -1041,59 +1072,86 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   if (staged)
     CKD_CUDA(cudaFuncSetAttribute(k_scatter<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scatter_smem(D)));
-  // pinned word for the per-level readback of (next open count, next working size)
-  static thread_local int64_t* level_tot = nullptr;
-  if (!level_tot) CKD_CUDA(cudaMallocHost((void**)&level_tot, sizeof(int64_t)));
+  // pinned word for the readback of the level state
+  static thread_local int4* level_st = nullptr;
+  if (!level_st) CKD_CUDA(cudaMallocHost((void**)&level_st, sizeof(int4)));
+  // Levels run ahead of the host: a chunk of up to kRunAhead levels is launched
+  // with grids sized by bounds known at the last readback (the working set never
+  // grows; a level has at most twice the previous level's open nodes and at most
+  // nw / (leaf + 1) of them), every kernel reads the exact counts from the
+  // device state and idles past them, and the host reads the state once per
+  // chunk.  Levels after the last open node are no-ops.
+  constexpr int kRunAhead = 6;
   int32_t n_nodes = T;
-  int m = (int)roots.size();
-  int alist = 0;  // open list buffer of this level
-  int level = 0;
+  int64_t m = (int64_t)roots.size();
+  *level_st = make_int4((int32_t)m, (int32_t)nw, n_nodes, 0);
+  CKD_CUDA(cudaMemcpyAsync(B.lst, level_st, sizeof(int4), cudaMemcpyHostToDevice, s));
+  int depth_levels = 0;
+  int par = 0;    // state slot of the next level
+  int alist = 0;  // open list buffer of the next level
+  int level = 0;  // levels launched
   while (m > 0) {
     if (level >= kMaxLevels) {
       dev_free(Ldev, s);
       return fail(CKD_ERR_DEPTH, "tree depth exceeds the build's level cap (8192 levels)");
     }
-    CKD_TRY(ensure_node_cap(B, (int64_t)n_nodes + 2 * (int64_t)m, s));
-    const int32_t* act = B.act[alist];
-    const unsigned gm = (unsigned)cdiv(m, 128);
-    const unsigned ntw = (unsigned)cdiv(nw, kTile);
-    if (level > 0) {  // the roots' boxes come from the validation pass
-      k_seg_box<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], n, nw, B.keys);
-      CKD_LAUNCH_CHECK();
+    int64_t mb[kRunAhead];
+    mb[0] = m;
+    int64_t grow = 2 * m;
+    int S = 1;
+    for (int c = 1; c < kRunAhead && level + c < kMaxLevels; ++c) {
+      mb[c] = std::min<int64_t>(2 * mb[c - 1], nw / (leaf + 1));
+      if (n_nodes + grow + 2 * mb[c] > B.cap) break;
+      grow += 2 * mb[c];
+      S = c + 1;
     }
-    k_decide<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.box, B.keys, B.mode, B.ext, B.wst,
-                                   B.frec);
-    CKD_LAUNCH_CHECK();
-    k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.frec, B.ext, n, nw, B.tile_sum, B.pstart,
-                                B.pend, B.flags);
-    CKD_LAUNCH_CHECK();
-    CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
-    k_children<D><<<gm, 128, 0, s>>>(act, m, B.meta, B.cell, B.pstart, B.pend, B.tile_off, B.wst,
-                                     B.mode, B.ext, B.nleft, B.pbase, B.keys, n_nodes, leaf,
-                                     B.nxt_cnt, B.scal + 1);
-    CKD_LAUNCH_CHECK();
-    CKD_TRY(scan_i64(B.nxt_cnt, B.nxt_off, m, s));
-    k_next_list<<<gm, 128, 0, s>>>(act, m, B.meta, B.nxt_off, leaf, B.mode, B.ext, B.nleft, B.pbase,
-                                   B.act[1 - alist], B.wst, B.srec);
-    CKD_LAUNCH_CHECK();
-    if (staged)
-      k_scatter<D, true><<<ntw, kBT, scatter_smem(D), s>>>(
-          B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off, B.flags, n, nw, B.X[1 - cur],
-          B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
-    else
-      k_scatter<D, false><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off,
-                                              B.flags, n, nw, B.X[1 - cur], B.I[1 - cur],
-                                              B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
-    CKD_LAUNCH_CHECK();
-    CKD_CUDA(cudaMemcpyAsync(level_tot, B.nxt_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CKD_TRY(ensure_node_cap(B, (int64_t)n_nodes + grow, s));
+    const unsigned ntw = (unsigned)cdiv(nw, kTile);
+    for (int c = 0; c < S; ++c, ++level) {
+      const int4* st = B.lst + par;
+      int4* st_next = B.lst + (1 - par);
+      const int32_t* act = B.act[alist];
+      const int mbi = (int)std::max<int64_t>(1, mb[c]);
+      const unsigned gm = (unsigned)cdiv(mbi, 128);
+      if (level > 0) {  // the roots' boxes come from the validation pass
+        k_seg_box<D><<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], n, nw, B.keys, st);
+        CKD_LAUNCH_CHECK();
+      }
+      k_decide<D><<<gm, 128, 0, s>>>(act, st, B.meta, B.cell, B.box, B.keys, B.mode, B.ext, B.wst,
+                                     B.frec);
+      CKD_LAUNCH_CHECK();
+      k_flags<<<ntw, kBT, 0, s>>>(B.X[cur], B.NID[cur], B.frec, B.ext, n, st, B.tile_sum,
+                                  B.pstart, B.pend, B.flags);
+      CKD_LAUNCH_CHECK();
+      CKD_TRY(scan_i32(B.tile_sum, B.tile_off, ntw, s));
+      k_children<D><<<gm, 128, 0, s>>>(act, st, mbi, B.meta, B.cell, B.pstart, B.pend, B.tile_off,
+                                       B.wst, B.mode, B.ext, B.nleft, B.pbase, B.keys, leaf,
+                                       B.nxt_cnt, B.scal + 1);
+      CKD_LAUNCH_CHECK();
+      CKD_TRY(scan_i64(B.nxt_cnt, B.nxt_off, mbi, s));
+      k_next_list<<<gm, 128, 0, s>>>(act, st, st_next, mbi, B.meta, B.nxt_off, leaf, B.mode, B.ext,
+                                     B.nleft, B.pbase, B.act[1 - alist], B.wst, B.srec);
+      CKD_LAUNCH_CHECK();
+      if (staged)
+        k_scatter<D, true><<<ntw, kBT, scatter_smem(D), s>>>(
+            B.X[cur], B.I[cur], B.NID[cur], B.srec, B.tile_off, B.flags, n, st, B.X[1 - cur],
+            B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids, B.scal + 1);
+      else
+        k_scatter<D, false><<<ntw, kBT, 0, s>>>(B.X[cur], B.I[cur], B.NID[cur], B.srec,
+                                                B.tile_off, B.flags, n, st, B.X[1 - cur],
+                                                B.I[1 - cur], B.NID[1 - cur], t->pts, t->ids,
+                                                B.scal + 1);
+      CKD_LAUNCH_CHECK();
+      cur = 1 - cur;
+      alist = 1 - alist;
+      par = 1 - par;
+    }
+    CKD_CUDA(cudaMemcpyAsync(level_st, B.lst + par, sizeof(int4), cudaMemcpyDeviceToHost, s));
     CKD_CUDA(cudaStreamSynchronize(s));
-    const int64_t tot = *level_tot;
-    n_nodes += 2 * m;
-    m = (int)(tot >> 32);
-    nw = tot & 0xffffffffll;
-    cur = 1 - cur;
-    alist = 1 - alist;
-    ++level;
+    m = level_st->x;
+    nw = level_st->y;
+    n_nodes = level_st->z;
+    depth_levels = level_st->w;
   }
   int32_t err = 0;
   CKD_CUDA(cudaMemcpyAsync(&err, B.scal + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1103,7 +1161,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
                                                              B.box);
   CKD_LAUNCH_CHECK();
   t->n_nodes = n_nodes;
-  t->depth = level;
+  t->depth = depth_levels;
   CKD_CUDA(dev_alloc((void**)&t->meta, sizeof(NodeMeta) * n_nodes, s));
   CKD_CUDA(dev_alloc((void**)&t->box, sizeof(double) * 2 * D * n_nodes, s));
   CKD_CUDA(dev_alloc((void**)&t->cell, sizeof(double) * 2 * D * n_nodes, s));
