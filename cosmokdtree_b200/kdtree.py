@@ -112,21 +112,21 @@ def _queries(tree: KDTree, target) -> tuple[torch.Tensor, bool]:
     if dev:
         q = target.to(device=f"cuda:{tree.device}", dtype=torch.float64)
     else:
-        q = torch.from_numpy(np.ascontiguousarray(np.array(target, dtype=np.float64, copy=False,
-                                                           ndmin=1)))
+        q = torch.from_numpy(np.ascontiguousarray(np.atleast_1d(np.asarray(target,
+                                                                           dtype=np.float64))))
     if q.dim() == 1:
         q = q.reshape(1, -1)
     if q.dim() != 2 or q.shape[1] != tree.d:
         raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
                                "target dimensionality does not match the tree")
-    if tree.periodic and q.shape[0] > 0:
+    if not dev:
+        q = q.pin_memory().to(f"cuda:{tree.device}", non_blocking=True)
+    if tree.periodic and q.shape[0] > 0:  # checked on the device
         half = torch.as_tensor(tree.boxsize / 2.0, dtype=torch.float64, device=q.device)
         bad = (q < -half) | (q > half) | torch.isnan(q)
         if bool(bad.any()):
             raise CKDArgumentError(_lib.CKD_ERR_OUT_OF_BOX,
                                    "periodic tree: query points must lie in [-L/2, L/2]")
-    if not dev:
-        q = q.pin_memory().to(f"cuda:{tree.device}", non_blocking=True)
     return q.contiguous(), dev
 
 
@@ -225,9 +225,56 @@ def knn_search_batch(tree: KDTree, target, k, sorted=True):
     return dist, idx
 
 
+_PIPE_MIN_ROWS = 1 << 20  # host queries from which the search and the copy-back overlap
+_PIPE_CHUNKS = 8
+
+
+def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool):
+    """Host queries, host results: the queries go to the device at once, then the
+    search runs in row chunks on the current stream while a second stream copies
+    each finished chunk's results into the pinned host arrays (two device buffers in
+    flight), so the result transfer overlaps the search."""
+    q, _ = _queries(tree, target)
+    nq = q.shape[0]
+    rows = -(-nq // _PIPE_CHUNKS)
+    dist_h = torch.empty((nq, k), dtype=torch.float64, pin_memory=True)
+    idx_h = torch.empty((nq, k), dtype=torch.int64, pin_memory=True)
+    comp = torch.cuda.current_stream()
+    copy = torch.cuda.Stream()
+    bufs = [(torch.empty((rows, k), dtype=torch.float64, device=q.device),
+             torch.empty((rows, k), dtype=torch.int64, device=q.device)) for _ in range(2)]
+    done = [None, None]
+    L = _lib.load()
+    for c, r0 in enumerate(range(0, nq, rows)):
+        r1 = min(nq, r0 + rows)
+        b = c % 2
+        if done[b] is not None:
+            comp.wait_event(done[b])  # the buffer's previous copy has finished
+        db, ib = bufs[b]
+        check(L.ckd_knn(tree.handle, _ptr(q[r0:r1]), r1 - r0, k, int(bool(sorted)), _ptr(db),
+                        _ptr(ib), ctypes.c_void_p(comp.cuda_stream)))
+        ready = torch.cuda.Event()
+        ready.record(comp)
+        copy.wait_event(ready)
+        with torch.cuda.stream(copy):
+            dist_h[r0:r1].copy_(db[: r1 - r0], non_blocking=True)
+            idx_h[r0:r1].copy_(ib[: r1 - r0], non_blocking=True)
+        done[b] = torch.cuda.Event()
+        done[b].record(copy)
+    copy.synchronize()
+    comp.wait_stream(copy)
+    return dist_h.numpy(), idx_h.numpy()
+
+
 def knn_search(tree: KDTree, target, k, sorted=True):
     """k nearest neighbours (kdtree.py:41-53).  Returns (dist, idx), each (ntar, k):
     numpy arrays for host input, CUDA tensors for CUDA-tensor input."""
+    if not _on_device(target):
+        k = _check_k(k)
+        nq = np.shape(target)[0] if np.ndim(target) == 2 else 1
+        if nq >= _PIPE_MIN_ROWS:
+            with torch.cuda.device(tree.device):
+                return _knn_host_pipelined(tree, target, k, sorted)
     dist, idx = knn_search_batch(tree, target, k, sorted)
     if _on_device(target):
         return dist, idx

@@ -443,3 +443,21 @@ def test_gpu_knn_multi_k(gpu, oracle):
     np.testing.assert_array_equal(np.sort(it.cpu().numpy(), 1), np.sort(i, 1))
     with pytest.raises(AssertionError):
         gpu.kdtree.knn_search_multi_k(t, Q[:3], [1, 0, 2])
+
+
+def test_gpu_knn_host_pipeline(gpu):
+    """Host queries from 2^20 rows take the chunked path (search and copy-back
+    overlapped on two streams); results equal the device path's."""
+    import torch
+    kd = gpu.kdtree
+    rng = np.random.default_rng(41)
+    P = rng.random((300_000, 3)) - 0.5
+    Q = rng.random(((1 << 20) + 77, 3)) - 0.5
+    t = kd.build_kdtree(P, boxsize=1.0)
+    d, i = kd.knn_search(t, Q, 8)
+    assert isinstance(d, np.ndarray) and d.shape == (len(Q), 8)
+    dd, ii = kd.knn_search_batch(t, torch.from_numpy(Q).cuda(), 8)
+    np.testing.assert_array_equal(i, ii.cpu().numpy())
+    np.testing.assert_array_equal(d, dd.cpu().numpy())
+    with pytest.raises(AssertionError):
+        kd.knn_search(t, np.full((1 << 20, 3), 0.75), 4)  # outside the periodic box
