@@ -229,11 +229,17 @@ _PIPE_MIN_ROWS = 1 << 20  # host queries from which the search and the copy-back
 _PIPE_CHUNKS = 8
 
 
-def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool):
+def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool, search=None):
     """Host queries, host results: the queries go to the device at once, then the
     search runs in row chunks on the current stream while a second stream copies
     each finished chunk's results into the pinned host arrays (two device buffers in
-    flight), so the result transfer overlaps the search."""
+    flight), so the result transfer overlaps the search.  ``search(q, n, dist, idx,
+    stream)`` runs one chunk (default: ckd_knn)."""
+    L = _lib.load()
+    if search is None:
+        def search(qc, n, db, ib, st):
+            check(L.ckd_knn(tree.handle, _ptr(qc), n, k, int(bool(sorted)), _ptr(db), _ptr(ib),
+                            st))
     q, _ = _queries(tree, target)
     nq = q.shape[0]
     rows = -(-nq // _PIPE_CHUNKS)
@@ -244,15 +250,13 @@ def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool):
     bufs = [(torch.empty((rows, k), dtype=torch.float64, device=q.device),
              torch.empty((rows, k), dtype=torch.int64, device=q.device)) for _ in range(2)]
     done = [None, None]
-    L = _lib.load()
     for c, r0 in enumerate(range(0, nq, rows)):
         r1 = min(nq, r0 + rows)
         b = c % 2
         if done[b] is not None:
             comp.wait_event(done[b])  # the buffer's previous copy has finished
         db, ib = bufs[b]
-        check(L.ckd_knn(tree.handle, _ptr(q[r0:r1]), r1 - r0, k, int(bool(sorted)), _ptr(db),
-                        _ptr(ib), ctypes.c_void_p(comp.cuda_stream)))
+        search(q[r0:r1], r1 - r0, db, ib, ctypes.c_void_p(comp.cuda_stream))
         ready = torch.cuda.Event()
         ready.record(comp)
         copy.wait_event(ready)
