@@ -63,6 +63,10 @@ STRUCT_CASES = [
     ("d8_periodic", 8000, 8, True, 16),
     ("tiny", 7, 3, False, 16),
     ("root_split", 17, 3, False, 16),
+    # odd n: the build's scalar (non-vector, unstaged) paths at every level
+    ("uniform3d_odd", 20001, 3, False, 16),
+    ("periodic_clustered_odd", 30001, 3, True, 8),
+    ("d4_odd", 12345, 4, True, 4),
 ]
 
 
