@@ -36,7 +36,7 @@ _KEY_VARIANT, _KEY_BPS, _KEY_WPB, _KEY_ORDER = 0, 1, 2, 6
 
 DEFAULT_GRID = {
     "leaf": (8, 16, 32),
-    "variant": (7, 8, 3, 2),
+    "variant": (9, 7, 8),
     "warps_per_block": (1, 2, 4),
     "blocks_per_sm": (0,),
     "order": (0,),

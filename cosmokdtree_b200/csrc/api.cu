@@ -35,16 +35,14 @@ int knn_variant() { return g_knn_variant.load(std::memory_order_relaxed); }
 static std::atomic<int> g_knn_bps{0}, g_knn_wpb{2};
 int knn_blocks_per_sm() { return g_knn_bps.load(std::memory_order_relaxed); }
 int knn_warps_per_block() { return g_knn_wpb.load(std::memory_order_relaxed); }
-static std::atomic<int> g_learned_kernel{3}, g_gather_wpb{2};
+static std::atomic<int> g_learned_kernel{3};
 int learned_kernel() { return g_learned_kernel.load(std::memory_order_relaxed); }
-int gather_warps_per_block() { return g_gather_wpb.load(std::memory_order_relaxed); }
 static std::atomic<int> g_order_mode{0};
 int query_order_mode() { return g_order_mode.load(std::memory_order_relaxed); }
 static std::atomic<int> g_mlp_tc{1};
 bool mlp_tensor_cores() { return g_mlp_tc.load(std::memory_order_relaxed) != 0; }
 static std::atomic<int> g_box_warp{1};
 bool box_warp_enabled() { return g_box_warp.load(std::memory_order_relaxed) != 0; }
-void set_knn_bucket_alpha(float a);
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ------------------------------------------------------------ kernel timing
@@ -473,7 +471,8 @@ int64_t ckd_launch_count(void) { return g_launches.load(); }
 ckd_status ckd_knn_stats(int enable, int64_t* out8) { return knn_stats(enable, out8); }
 
 ckd_status ckd_set_knn_variant(int variant) {
-  if (variant < 0 || variant > 8) return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0..8");
+  if (!(variant == 0 || variant == 1 || variant == 7 || variant == 8 || variant == 9))
+    return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0, 1, 7, 8 or 9");
   g_knn_variant.store(variant);
   return CKD_OK;
 }
@@ -503,17 +502,10 @@ ckd_status ckd_set_tuning(int key, int value) {
       if (value < 1 || value > 8) return fail(CKD_ERR_BAD_ARG, "warps per block must be 1..8");
       g_knn_wpb.store(value);
       return CKD_OK;
-    case 3:
-      if (value < 10 || value > 1000) return fail(CKD_ERR_BAD_ARG, "bucket radius factor must be 10..1000");
-      set_knn_bucket_alpha(value / 100.0f);
-      return CKD_OK;
     case 4:
-      if (value < 0 || value > 3) return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0..3");
+      if (!(value == 0 || value == 3 || value == 4))
+        return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0, 3 or 4");
       g_learned_kernel.store(value);
-      return CKD_OK;
-    case 5:
-      if (value < 1 || value > 4) return fail(CKD_ERR_BAD_ARG, "gather warps per block must be 1..4");
-      g_gather_wpb.store(value);
       return CKD_OK;
     case 6:
       if (value < 0 || value > 2) return fail(CKD_ERR_BAD_ARG, "query ordering must be 0, 1 or 2");
@@ -527,6 +519,7 @@ ckd_status ckd_set_tuning(int key, int value) {
       if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "box kernel choice must be 0 or 1");
       g_box_warp.store(value);
       return CKD_OK;
+
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
 }

@@ -785,42 +785,30 @@ __global__ void k_pts64(const double* __restrict__ Pf, int64_t n, double4* __res
     P64[p * NV + h] = make_double4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
-// Each point relative to its leaf's box centre, rounded to FP32, packed in float4s.
+// Absolute coordinates rounded to FP32, packed in float4s (zero padded).
 template <int D>
-__global__ void k_pts32(const NodeMeta* __restrict__ meta, int32_t n_nodes, int leaf,
-                        const double* __restrict__ box, const double* __restrict__ Pf, int64_t n,
-                        float4* __restrict__ P32) {
+__global__ void k_pts32(const double* __restrict__ Pf, int64_t n, float4* __restrict__ P32) {
   constexpr int NV = (D + 3) / 4;
-  int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n_nodes) return;
-  NodeMeta m = meta[a];
-  if (m.left >= 0) return;
-  double c[D];
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  float v[4 * NV];
 #pragma unroll
-  for (int j = 0; j < D; ++j)
-    c[j] = leaf_centre(box[(int64_t)a * 2 * D + 2 * j], box[(int64_t)a * 2 * D + 2 * j + 1]);
-  for (int i = 0; i < m.count; ++i) {
-    int64_t p = (int64_t)m.start + i;
-    float v[4 * NV];
+  for (int j = 0; j < 4 * NV; ++j) v[j] = j < D ? __double2float_rn(Pf[(int64_t)(j < D ? j : 0) * n + p]) : 0.0f;
 #pragma unroll
-    for (int j = 0; j < 4 * NV; ++j)
-      v[j] = j < D ? __double2float_rn(__dsub_rn(Pf[(int64_t)j * n + p], c[j < D ? j : 0])) : 0.0f;
-#pragma unroll
-    for (int h = 0; h < NV; ++h)
-      P32[p * NV + h] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
-  }
+  for (int h = 0; h < NV; ++h)
+    P32[p * NV + h] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
-// Bottom-up search records: inward-rounded FP32 cells, FP64 leaf centres, and for
-// each internal node the child-pair record (both children's outward FP32 boxes,
-// ids and leaf flags) so one load serves a whole expansion.
+// Search records: inward-rounded FP32 cells, FP64 leaf centres, and for each
+// internal node the child-pair record (both children's outward FP32 boxes, ids,
+// leaf flags and position ranges) so one load serves a whole expansion.
 template <int D>
 __global__ void k_search_records(const NodeMeta* __restrict__ meta, int32_t n_nodes,
                                  const double* __restrict__ box, const double* __restrict__ cell,
                                  float4* __restrict__ pair, float* __restrict__ cell32,
                                  double* __restrict__ centre) {
   constexpr int NV = (D + 3) / 4;
-  constexpr int PF = 4 * NV + 1;
+  constexpr int PF = pair_f4(D);
   int32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n_nodes) return;
   NodeMeta m = meta[a];
@@ -852,9 +840,11 @@ __global__ void k_search_records(const NodeMeta* __restrict__ meta, int32_t n_no
           make_float4(hi[4 * h], hi[4 * h + 1], hi[4 * h + 2], hi[4 * h + 3]);
     }
   }
-  int4 info = make_int4(m.left, m.left + 1, meta[m.left].left < 0 ? 1 : 0,
-                        meta[m.left + 1].left < 0 ? 1 : 0);
+  const NodeMeta ml = meta[m.left], mr = meta[m.left + 1];
+  int4 info = make_int4(m.left, m.left + 1, ml.left < 0 ? 1 : 0, mr.left < 0 ? 1 : 0);
   rec[4 * NV] = *reinterpret_cast<float4*>(&info);
+  int4 range = make_int4(ml.start, ml.count, mr.start, mr.count);
+  rec[4 * NV + 1] = *reinterpret_cast<float4*>(&range);
 }
 
 // roots: node t = root of tree t (positions off[t] .. off[t+1]-1)
@@ -1183,10 +1173,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   CKD_CUDA(dev_alloc((void**)&t->pts64, sizeof(double4) * NV * n, s));
   k_pts64<D><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(t->pts, n, t->pts64);
   CKD_LAUNCH_CHECK();
-  k_box32<D><<<(unsigned)cdiv((int64_t)n_nodes * 2 * D, 256), 256, 0, s>>>(t->box, n_nodes, t->box32);
+  k_pts32<D><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(t->pts, n, t->pts32);
   CKD_LAUNCH_CHECK();
-  k_pts32<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(t->meta, n_nodes, leaf, t->box, t->pts, n,
-                                                          t->pts32);
+  k_box32<D><<<(unsigned)cdiv((int64_t)n_nodes * 2 * D, 256), 256, 0, s>>>(t->box, n_nodes, t->box32);
   CKD_LAUNCH_CHECK();
   CKD_CUDA(dev_alloc((void**)&t->pair, sizeof(float4) * pair_f4(D) * n_nodes, s));
   CKD_CUDA(dev_alloc((void**)&t->cell32, sizeof(float) * 2 * D * n_nodes, s));

@@ -37,17 +37,15 @@ void note_launch();
     if (_s != CKD_OK) return _s;         \
   } while (0)
 
-// kNN kernel choice: 0 automatic, 1 FP64-only traversal, 2 FP32-screened traversal
+// kNN kernel choice (ckd_set_knn_variant): 0 automatic, 1 FP64 packet traversal,
+// 7/8 per-lane compact heap, 9 warp-converged
 int knn_variant();
 // tuning knobs (see ckd_set_tuning): blocks-per-SM cap (0 = none), warps per block
 int knn_blocks_per_sm();
 int knn_warps_per_block();
 // learned-bound search kernel: 0 bounded per-lane with compact heap (k_knn_lane2),
-// 1 warp gather, 2 bounded per-lane with the wide heap (k_knn_lane), 3 as 0 with
-// child-pair-record descent (default);
-// warps per block of the gather kernel
+// 3 as 0 with child-pair-record descent (default), 4 bounded warp-converged
 int learned_kernel();
-int gather_warps_per_block();
 // query leaf ordering before a search: 0 automatic, 1 always, 2 never
 int query_order_mode();
 // learned-bound network inference on the tensor cores (tcgen05) instead of FP32 FMAs
@@ -89,8 +87,10 @@ struct TreeView {
   const double* cell;        // [n_nodes][2d] sliding-midpoint cell (reference node bounds)
   const double* pts;         // SoA [d][n], leaf order
   const int32_t* ids;        // [n] original index per leaf-ordered point
-  // FP32 screening copies (see leaf_frame): node boxes rounded outwards, and
-  // each point relative to its leaf's box centre, 1 (d <= 4) or 2 float4 per point
+  // FP32 screening copies: node boxes rounded outwards, and each point's
+  // absolute coordinates rounded to FP32 (zero padded), 1 (d <= 4) or 2 float4
+  // per point, for screens whose error bound depends only on the query and the
+  // coordinate range
   const float* box32;        // [n_nodes][2d]
   const float4* pts32;       // [n][(d + 3) / 4]
   // the FP64 points again, one 32-byte (d <= 4) or 64-byte record per point, so an
@@ -103,10 +103,11 @@ struct TreeView {
   const double* centre;      // [n_nodes][d] leaf centres (leaf_centre of the FP64 box)
 };
 
-// Child-pair record of an internal node, (4 * NV + 1) float4s with NV = (d+3)/4:
+// Child-pair record of an internal node, (4 * NV + 2) float4s with NV = (d+3)/4:
 // left lo[NV], left hi[NV], right lo[NV], right hi[NV], then int4 {left node,
-// right node, left is-leaf, right is-leaf}.
-__host__ __device__ constexpr int pair_f4(int d) { return 4 * ((d + 3) / 4) + 1; }
+// right node, left is-leaf, right is-leaf}, then int4 {left start, left count,
+// right start, right count} (the children's ranges of leaf-ordered positions).
+__host__ __device__ constexpr int pair_f4(int d) { return 4 * ((d + 3) / 4) + 2; }
 
 // Leaf frame used by the FP32 screen: centre c = 0.5 * (lo + hi) of the leaf's
 // FP64 box (the same separately rounded operations when the FP32 copy is made

@@ -2,7 +2,7 @@
 //
 // The file holds the handle's scalars and every device array as a raw copy, so a
 // loaded tree is bit-for-bit the tree that was saved and returns identical
-// results without rebuilding.  Layout (little-endian): magic "CKDTREE1", a header
+// results without rebuilding.  Layout (little-endian): magic "CKDTREE2", a header
 // of fixed-size scalars, the tree offsets (n_trees + 1 int64), then each array as
 // (int64 byte count, bytes) in a fixed order.  No counterpart in the reference,
 // which rebuilds its tree on every run.
@@ -82,7 +82,7 @@ ckd_status ckd_tree_save(const ckd_tree* tree, const char* path) {
   h.screen_ok = t->screen_ok ? 1 : 0;
   std::memcpy(h.L, t->L, sizeof(h.L));
   std::memcpy(h.slack, t->slack, sizeof(h.slack));
-  bool ok = fwrite("CKDTREE1", 1, 8, fh.f) == 8 && fwrite(&h, sizeof(h), 1, fh.f) == 1 &&
+  bool ok = fwrite("CKDTREE2", 1, 8, fh.f) == 8 && fwrite(&h, sizeof(h), 1, fh.f) == 1 &&
             fwrite(t->tree_off.data(), sizeof(int64_t), t->tree_off.size(), fh.f) ==
                 t->tree_off.size();
   std::vector<unsigned char> buf;
@@ -104,7 +104,7 @@ ckd_status ckd_tree_load(const char* path, ckd_tree** out) {
   if (!fh.f) return fail(CKD_ERR_BAD_ARG, std::string("cannot open ") + path);
   char magic[8];
   Header h;
-  if (fread(magic, 1, 8, fh.f) != 8 || std::memcmp(magic, "CKDTREE1", 8) != 0 ||
+  if (fread(magic, 1, 8, fh.f) != 8 || std::memcmp(magic, "CKDTREE2", 8) != 0 ||
       fread(&h, sizeof(h), 1, fh.f) != 1)
     return fail(CKD_ERR_BAD_ARG, std::string(path) + " is not a saved tree");
   if (h.d < 1 || h.d > CKD_MAX_D || h.n < 1 || h.n_trees < 1 || h.n_nodes < 1 || h.n_trees > h.n)

@@ -102,39 +102,38 @@ ckd_status ckd_knn_ordered(const ckd_tree* tree, const double* q_dev, int64_t nq
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t ckd_launch_count(void);
 
-/* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (7
+/* Process-wide kNN kernel choice (no reference counterpart): 0 = automatic (8
  * when k <= 64, the coordinates allow the FP32 screen and the tree is shallow
- * enough, else 2), 1 = FP64-only packet traversal, 2 = FP32-screened packet
- * traversal, 3 = per-lane traversal with 12-byte heap entries, 4 = bottom-up
- * per-lane search, 5 = persistent per-lane search, 6 = warp per bucket with a
- * density radius, 7 = per-lane traversal with 8-byte heap entries (FP32 key +
- * position, exact tie resolution), 8 = 7 expanding nodes from child-pair records.
- * Every variant returns the same exact result. */
+ * enough; 1 otherwise), 1 = FP64 packet
+ * traversal, 7 = per-lane traversal with 8-byte heap entries (FP32 key +
+ * position, exact tie resolution), 8 = 7 expanding nodes from child-pair records,
+ * 9 = warp-converged search (a warp walks the tree once for 32 queries adjacent
+ * in leaf order and screens each visited leaf for all of them).  Every variant
+ * returns the same exact result. */
 ckd_status ckd_set_knn_variant(int variant);
 
 /* Process-wide launch tuning of the search kernels (no reference counterpart;
  * set by the autotuner).  key 0: kNN variant (as ckd_set_knn_variant);
- * key 1: cap on resident blocks per SM for the kNN kernel (0 = as many as fit,
- * fewer leaves more of the unified L1 to the data cache); key 2: warps per block
- * of the kNN kernel (1..8, default 2; the per-lane kernels use at most 4); key 3:
- * radius factor of the warp-per-bucket kNN search in hundredths (default 150 =
- * 1.5x the density estimate); key 4: search kernel of ckd_knn_learned (0 = bounded
- * per-lane traversal with 8-byte heap entries; 1 = warp gather; 2 = bounded
- * per-lane with 12-byte entries; 3 = 0 with child-pair-record descent, default);
- * key 5: warps per block of the warp-gather kernel (1..4, default 2);
- * key 6: ordering of queries by leaf before kNN and ball searches (0 = automatic,
- * default; 1 = always; 2 = never); key 7: inference of the learned-bound network
- * (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on BF16 activations, default);
- * key 8: box search of up to 32768 boxes per call (1 = a warp per box, frontier
- * expanded a level at a time, default; 0 = a lane per box). */
+ * key 1: cap on resident blocks per SM for the per-lane kNN kernel (0 = as many
+ * as fit); key 2: warps per block of the per-lane kNN kernel (1..8, default 2,
+ * at most 4 used); key 4: search kernel of ckd_knn_learned (0 = bounded per-lane
+ * traversal; 3 = 0 with child-pair-record descent, default; 4 = bounded
+ * warp-converged search); key 6: ordering of queries by leaf before kNN and ball
+ * searches (0 = automatic, default; 1 = always; 2 = never); key 7: inference of
+ * the learned-bound network (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on
+ * BF16 activations, default); key 8: box search of up to 32768 boxes per call
+ * (1 = a warp per box, frontier expanded a level at a time, default; 0 = a lane
+ * per box). */
 ckd_status ckd_set_tuning(int key, int value);
 
-/* Traversal statistics of the FP32-screened kNN kernel (diagnostics, no reference
+/* Traversal statistics of the kNN kernels (diagnostics, no reference
  * counterpart).  Copies the counters accumulated since the previous call into
- * out8 (if not NULL; 8 entries: node pops, needed pops, leaf visits, points
- * screened, warp insert rounds, FP64 evaluations, heap inserts, lanes active on
- * leaf visits), clears them, and turns collection on (enable=1) or off.
- * Synchronises the device. */
+ * out8 (if not NULL), clears them, and turns collection on (enable=1) or off.
+ * Warp-converged kernel: [0] node expansions, [1] stack pops, [2] leaf scans,
+ * [3] points screened (per warp), [4] own leaves scanned first, [5] screen passes
+ * (FP64 evaluations, per query), [6] heap inserts (per query), [7] climb steps.
+ * Per-lane kernel: [0] node expansions, [2] leaf visits, [3] points screened,
+ * [5] screen passes, [6] heap inserts (all per query).  Synchronises the device. */
 ckd_status ckd_knn_stats(int enable, int64_t* out8);
 
 /* Kernel timing (diagnostics, no reference counterpart).  With enable=1 the kNN

@@ -118,14 +118,19 @@ KNN_CASES = [
 ]
 
 
-@pytest.fixture(params=[1, 2, 3, 4, 5, 6, 7, 8],
-                ids=["fp64", "screened", "lane", "bottom_up", "persistent", "bucket",
-                     "lane_compact", "lane_compact_pair"])
+@pytest.fixture(params=[1, 7, 8, 9, 0],
+                ids=["fp64", "lane_compact", "lane_compact_pair", "warp", "auto"])
 def knn_variant(request, gpu):
+    """Every kNN kernel of the product.  The warp-converged kernel (9) needs the
+    queries in leaf order, so its case forces the ordering pass (tuning key 6)."""
     from cosmokdtree_b200 import _lib
-    _lib.check(_lib.load().ckd_set_knn_variant(request.param))
+    L = _lib.load()
+    _lib.check(L.ckd_set_knn_variant(request.param))
+    if request.param == 9:
+        _lib.check(L.ckd_set_tuning(6, 1))
     yield request.param
-    _lib.load().ckd_set_knn_variant(0)
+    L.ckd_set_knn_variant(0)
+    L.ckd_set_tuning(6, 0)
 
 
 @pytest.mark.parametrize("name,n,d,periodic,leaf,nq,k", KNN_CASES)
