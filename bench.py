@@ -12,8 +12,11 @@ beforehand (untimed, like the tree build) on 10^6 exact k-th distances of a
 separate catalogue drawn with another seed.  Timing: CUDA events on
 the launching stream, barrier + synchronize around the timed region, max over
 ranks.  Inputs (tree ~0.6 GB, outputs 8.6 GB per step) are far larger than L2.
-Under torchrun each rank builds and searches its own catalogue (seed + rank) with
-no collective on the data path (weak scaling); rank 0 prints one JSON line.
+With --gpus N > 1 (one process per GPU: launched by torchrun, or relaunched under
+torchrun by this script when started plainly) every rank builds a replica of the
+same tree in its own HBM and searches a contiguous shard of the 2^24 queries
+(distributed.knn_sharded), with no collective on the data path: the job is fixed,
+so scaling is strong; rank 0 prints one JSON line.
 
 --impl reference times the reference algorithm's CPU implementation (the C++
 restatement in oracle/, OpenMP over queries like src/cosmokdtree2py.f90:132-141) on
@@ -185,8 +188,8 @@ def run_reference(args):
         "impl": "reference", "metric": "knn_queries_per_s", "value": value, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(samples) / len(samples), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(name),
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(name, args.gpus),
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
                          "sample": f"{m_step} random self-queries of the {n}-point catalogue "
                                    "per step, reference traversal (hyperplane DFS, periodic)"},
@@ -566,11 +569,48 @@ def run_multi(args):
     return 0
 
 
-def workload_config(name):
+def workload_config(name, world=1):
     n, k, periodic, leaf, seed = WORKLOADS[name]
     return {"workload": name, "n_points": n, "n_queries": n, "k": k, "sorted": True,
             "periodic": periodic, "leaf": leaf, "seed": seed, "dims": 3,
+            "parallelism": f"tree replica per GPU, {world} contiguous query shard(s)",
             "l2": "inputs larger than L2 (tree ~0.6 GB, outputs 8.6 GB per step)"}
+
+
+def build_roofline(tree, n, d, ms):
+    """Build roofline from the algorithmic bytes of a level-synchronous build: the
+    input read once (N·D·8), every point read and written once per level above its
+    leaf (Σ_p depth(p)·2·(D·8 + 4)), and the leaf-ordered write (N·(D·8 + 4))."""
+    ex = tree.export()
+    left, right, count, axis = ex["left"], ex["right"], ex["count"], ex["axis"]
+    depth = np.zeros(len(left), dtype=np.int64)
+    internal = np.nonzero(left >= 0)[0]
+    for _ in range(int(tree.depth) + 1):  # preorder parents precede children
+        depth[left[internal]] = depth[internal] + 1
+        depth[right[internal]] = depth[internal] + 1
+    leaves = axis < 0
+    point_levels = int((depth[leaves] * count[leaves]).sum())
+    rec = d * 8 + 4
+    alg = n * d * 8 + point_levels * 2 * rec + n * rec
+    peak, kind = measured_peaks()
+    a = alg / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+            "traffic": None, "alg_bytes": alg, "point_levels_per_point": point_levels / n,
+            "kernel": "whole build (all levels)", "peak_kind": kind}
+
+
+def launch_ranks(n_gpus):
+    """Relaunch this command under torchrun with one process per GPU (rendezvous on
+    127.0.0.1) and return its exit status."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n_gpus}", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -608,12 +648,18 @@ def main():
     if args.workload == "uniform_2p20_small":
         return run_small_uniform(args)
 
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        return launch_ranks(args.gpus)
     import torch
     import torch.distributed as dist
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        print(json.dumps({"error": f"--gpus {args.gpus} but WORLD_SIZE={world}: launch one "
+                                   "process per GPU"}))
+        return 2
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -639,7 +685,7 @@ def main():
         _lib.check(L.ckd_set_tuning(int(key), int(val)))
     name = args.workload
     n, k, periodic, leaf, seed = WORKLOADS[name]
-    P = make_points(name, seed_offset=rank)
+    P = make_points(name)  # the same catalogue on every rank: a tree replica per GPU
     box = [1.0, 1.0, 1.0] if periodic else None
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -678,6 +724,7 @@ def main():
         if it < n_builds - 1:
             tree.close()
     build_ms_v = allmax(float(np.mean(build_ms)))
+    build_roof = build_roofline(tree, n, 3, build_ms_v) if rank == 0 else None
     # the input's host-to-device copy (pinned host buffer), reported beside the build
     P_pin = torch.from_numpy(P).pin_memory()
     Pd2 = torch.empty_like(Pd)
@@ -690,9 +737,13 @@ def main():
     build_h2d_ms = allmax(e0.elapsed_time(e1))
     del P_pin, Pd2
 
-    # ---- kNN, inputs resident in HBM
-    nq = P.shape[0]
-    Q = Pd
+    # ---- kNN, inputs resident in HBM: every point of the catalogue is a query;
+    # this rank searches its contiguous shard [lo, hi) against its replica
+    from cosmokdtree_b200.distributed import knn_sharded, shard_bounds
+    n_all = P.shape[0]
+    lo, hi = shard_bounds(n_all, rank, world)
+    nq = hi - lo
+    Q = Pd[lo:hi]
     dist_t = torch.empty((nq, k), dtype=torch.float64, device="cuda")
     idx_t = torch.empty((nq, k), dtype=torch.int64, device="cuda")
     dist_l = torch.empty((nq, k), dtype=torch.float64, device="cuda")
@@ -701,8 +752,13 @@ def main():
     dlp, ilp = (ctypes.c_void_p(x.data_ptr()) for x in (dist_l, idx_l))
     nfb = ctypes.c_int64()
 
+    def search_into(t, q, kk, srt):
+        _lib.check(L.ckd_knn(t.handle, ctypes.c_void_p(q.data_ptr()), q.shape[0], kk, int(srt),
+                             dp, ip, sp))
+        return dist_t, idx_t
+
     def plain_step():
-        _lib.check(L.ckd_knn(tree.handle, qp, nq, k, 1, dp, ip, sp))
+        knn_sharded(tree, Pd, k, True, search=search_into)
 
     def learned_step():
         _lib.check(L.ckd_knn_learned(tree.handle, lb.handle, qp, nq, k, 1, dlp, ilp,
@@ -753,12 +809,12 @@ def main():
     # ---- learned bound: trained on a separate catalogue (seed + 2), 10^6 samples
     from cosmokdtree_b200.learned import LearnedBound
     t_tr = time.perf_counter()
-    P_tr = make_points(name, seed_offset=rank + 2)
+    P_tr = make_points(name, seed_offset=2)
     tree_tr = kdtree.build_kdtree(torch.from_numpy(P_tr).cuda(), leaf=leaf, boxsize=box)
-    rng_tr = np.random.default_rng(3 + rank)
+    rng_tr = np.random.default_rng(3)
     n_train = min(1_000_000, P_tr.shape[0])
     Q_tr = torch.from_numpy(P_tr[rng_tr.integers(0, P_tr.shape[0], n_train)]).cuda()
-    lb = LearnedBound(seed=rank)
+    lb = LearnedBound(seed=0)
     fit = lb.fit(tree_tr, Q_tr, k, epochs=30 if not args.profile else 4, batch=4096, lr=3e-3,
                  quantile=0.97)
     torch.cuda.synchronize()
@@ -775,8 +831,8 @@ def main():
     learned_kernel_ms = kernel_ms(learned_step)
     exact = bool(torch.equal(idx_l, idx_t) and torch.equal(dist_l, dist_t))
     exact = allmax(0.0 if exact else 1.0) == 0.0
-    plain_value = world * nq * args.steps / (plain_total / 1e3)
-    learned_value = world * nq * args.steps / (learned_total / 1e3)
+    plain_value = n_all * args.steps / (plain_total / 1e3)
+    learned_value = n_all * args.steps / (learned_total / 1e3)
     # headline: the default exact path (knn_search / ckd_knn); the learned-bound
     # search is reported beside it with its ratio
     value = plain_value
@@ -855,11 +911,12 @@ def main():
                 vals.append(e0.elapsed_time(e1))
         return allmax(float(np.mean(vals))), res
 
-    samp = np.random.default_rng(7).integers(0, nq, 20000)  # parity rows
-    e2e_learned_ms, res = e2e(lambda: lb.knn(tree, P, k, sorted=True))
-    hd, hi = res[0][samp], res[1][samp]
+    samp = np.random.default_rng(7).integers(0, nq, 20000)  # parity rows (of this shard)
+    Ph = P[lo:hi]
+    e2e_learned_ms, res = e2e(lambda: lb.knn(tree, Ph, k, sorted=True))
+    hd, hi_l = res[0][samp], res[1][samp]
     del res
-    e2e_ms_v, res = e2e(lambda: kdtree.knn_search(tree, P, k, sorted=True))
+    e2e_ms_v, res = e2e(lambda: kdtree.knn_search(tree, Ph, k, sorted=True))
     hd0, hi0 = res[0][samp], res[1][samp]
     del res
 
@@ -871,13 +928,13 @@ def main():
         t0 = time.perf_counter()
         otree = oracle.OracleTree(P, leaf, 1.0 if periodic else None, threads=threads)
         cpu_build_s = time.perf_counter() - t0
-        od, oi = otree.knn(P[samp], k)
-        parity = bool(np.array_equal(oi, hi) and np.array_equal(od, hd) and
+        od, oi = otree.knn(Ph[samp], k)
+        parity = bool(np.array_equal(oi, hi_l) and np.array_equal(od, hd) and
                       np.array_equal(oi, hi0) and np.array_equal(od, hd0))
         # ball parity on a sample: the count pass against the oracle's CSR
-        bo_o, _, _ = otree.ball_csr(P[samp[:5000]], radius)
+        bo_o, _, _ = otree.ball_csr(Ph[samp[:5000]], radius)
         ball_parity = bool(np.array_equal(np.diff(bo_o), counts[torch.from_numpy(samp[:5000]).cuda()].cpu().numpy()))
-        ab = otree.knn_algbytes(P[samp], k, od[:, -1] ** 2)
+        ab = otree.knn_algbytes(Ph[samp], k, od[:, -1] ** 2)
         bytes_per_q = ab["bytes"] / len(samp)
 
         def roof(ms, kernel):
@@ -895,13 +952,13 @@ def main():
         out = {
             "metric": "knn_queries_per_s", "value": value, "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(name),
+            "config": workload_config(name, world),
             "roofline": roof(plain_kernel_ms, "k_knn_lane2"),
             "cpu_baseline": cpu,
-            "e2e": {"value": world * nq / (e2e_ms_v / 1e3), "unit": "queries/s",
-                    "h2d_bytes_per_step": nq * 3 * 8, "d2h_bytes_per_step": nq * k * 16,
+            "e2e": {"value": n_all / (e2e_ms_v / 1e3), "unit": "queries/s",
+                    "h2d_bytes_per_step": n_all * 3 * 8, "d2h_bytes_per_step": n_all * k * 16,
                     "ms_per_step": e2e_ms_v},
             "gpu_launches": int(plain_launches),
             "clocks": clocks,
@@ -913,7 +970,7 @@ def main():
                         "gpu_launches": int(launches),
                         "roofline": roof(learned_kernel_ms,
                                          "k_mlp_radius + k_knn_lane2 (bounded) + rerun"),
-                        "e2e_queries_per_s": world * nq / (e2e_learned_ms / 1e3),
+                        "e2e_queries_per_s": n_all / (e2e_learned_ms / 1e3),
                         "train_s": train_s, "train_samples": fit["n_train"],
                         "train_catalogue_seed_offset": 2, "margin_log2": fit["margin"],
                         "holdout_rms_log2": fit["holdout_rms_log2"],
@@ -922,7 +979,7 @@ def main():
             "plain": {"value": plain_value, "ms_per_step": plain_total / args.steps,
                       "kernel_ms": plain_kernel_ms, "method": "knn_search / ckd_knn (default)"},
             "ball": {"radius": radius, "unit": "queries/s",
-                     "count_pass": {"queries": nq, "value": world * nq * args.steps /
+                     "count_pass": {"queries": n_all, "value": n_all * args.steps /
                                     (ball_count_total / 1e3),
                                     "ms_per_step": ball_count_total / args.steps,
                                     "total_hits": total_hits, "mean_hits": mean_hits},
@@ -933,7 +990,7 @@ def main():
                                          "gpu_launches": int(ball_launches)},
                      "count_parity_sample": ball_parity},
             "build": {"ms": build_ms_v, "mpts_per_s": n / (build_ms_v / 1e3) / 1e6,
-                      "input_h2d_ms": build_h2d_ms,
+                      "input_h2d_ms": build_h2d_ms, "roofline": build_roof,
                       "cpu_s": cpu_build_s, "cpu_mpts_per_s": n / cpu_build_s / 1e6,
                       "n_nodes": tree.n_nodes, "depth": tree.depth},
             "breakdown_ms": {"learned_step": float(np.mean(learned_steps)),

@@ -75,6 +75,7 @@ SIGNATURES = {
     "ckd_build": [_vp, _i64, _int, _int, _int, _pdbl, _int, _vp, ctypes.POINTER(_vp)],
     "ckd_free": [_vp],
     "ckd_release_cached_memory": [],
+    "ckd_pool_usage": [_pi64, _pi64],
     "ckd_tree_info": [_vp, _pi64, _pint, _pint, _pint, _pi32, _pi32, _pi32, _pint],
     "ckd_tree_export": [_vp, _pi32, _pdbl, _pi64, _pi64, _pi64, _pi64, _pdbl, _pdbl, _pi64],
     "ckd_knn": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],

@@ -93,11 +93,27 @@ static cudaError_t pool_for_current(cudaMemPool_t* out) {
   return cudaSuccess;
 }
 
+// Optional cap on the bytes the pool holds for callers at any time (tuning key 9,
+// MiB, 0 = none): an allocation that would take the pool's in-use bytes past it
+// fails as out of memory, so callers can bound the library's footprint (and the
+// allocation-failure paths can be exercised from the host).
+static std::atomic<int64_t> g_pool_cap{0};
+
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool;
   cudaError_t e = pool_for_current(&pool);
   if (e != cudaSuccess) return e;
   if (bytes == 0) bytes = 16;
+  const int64_t cap = g_pool_cap.load(std::memory_order_relaxed);
+  if (cap > 0) {
+    uint64_t used = 0;
+    e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (e != cudaSuccess) return e;
+    if ((int64_t)(used + bytes) > cap) {
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+  }
   return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 cudaError_t dev_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
@@ -348,6 +364,17 @@ ckd_status ckd_forest_ball_fill(const ckd_tree* t, const double* q, const int64_
                      stream);
 }
 
+ckd_status ckd_pool_usage(int64_t* used, int64_t* reserved) {
+  cudaMemPool_t pool;
+  CKD_CUDA(pool_for_current(&pool));
+  uint64_t u = 0, r = 0;
+  CKD_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+  CKD_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+  if (used) *used = (int64_t)u;
+  if (reserved) *reserved = (int64_t)r;
+  return CKD_OK;
+}
+
 ckd_status ckd_release_cached_memory(void) {
   cudaMemPool_t pool;
   CKD_CUDA(pool_for_current(&pool));
@@ -519,6 +546,10 @@ ckd_status ckd_set_tuning(int key, int value) {
       if (value < 0 || value > 1) return fail(CKD_ERR_BAD_ARG, "box kernel choice must be 0 or 1");
       g_box_warp.store(value);
       return CKD_OK;
+    case 9:
+      if (value < 0) return fail(CKD_ERR_BAD_ARG, "pool cap must be >= 0 MiB");
+      g_pool_cap.store((int64_t)value << 20);
+      return CKD_OK;
 
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
@@ -558,19 +589,25 @@ ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, i
   cudaStream_t s = (cudaStream_t)stream;
   double *dq = nullptr, *dd = nullptr;
   int64_t* di = nullptr;
-  CKD_CUDA(dev_alloc((void**)&dq, sizeof(double) * nq * t->d, s));
-  CKD_CUDA(dev_alloc((void**)&dd, sizeof(double) * nq * k, s));
-  CKD_CUDA(dev_alloc((void**)&di, sizeof(int64_t) * nq * k, s));
-  CKD_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * nq * t->d, cudaMemcpyHostToDevice, s));
-  ckd_status st = knn_run(t, dq, nq, k, sorted, dd, di, s);
+  ckd_status st = CKD_OK;
+  cudaError_t e = dev_alloc((void**)&dq, sizeof(double) * nq * t->d, s);
+  if (e == cudaSuccess) e = dev_alloc((void**)&dd, sizeof(double) * nq * k, s);
+  if (e == cudaSuccess) e = dev_alloc((void**)&di, sizeof(int64_t) * nq * k, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dq, q, sizeof(double) * nq * t->d, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) st = cuda_fail(e, "ckd_knn_host: device buffers");
+  if (st == CKD_OK) st = knn_run(t, dq, nq, k, sorted, dd, di, s);
   if (st == CKD_OK) {
-    CKD_CUDA(cudaMemcpyAsync(dist, dd, sizeof(double) * nq * k, cudaMemcpyDeviceToHost, s));
-    CKD_CUDA(cudaMemcpyAsync(idx, di, sizeof(int64_t) * nq * k, cudaMemcpyDeviceToHost, s));
+    e = cudaMemcpyAsync(dist, dd, sizeof(double) * nq * k, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(idx, di, sizeof(int64_t) * nq * k, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) st = cuda_fail(e, "ckd_knn_host: result copy");
   }
   dev_free(dq, s);
   dev_free(dd, s);
   dev_free(di, s);
-  CKD_CUDA(cudaStreamSynchronize(s));
+  e = cudaStreamSynchronize(s);
+  if (st == CKD_OK && e != cudaSuccess) st = cuda_fail(e, "ckd_knn_host");
   return st;
 }
 

@@ -775,17 +775,18 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
   unsigned blocks = (unsigned)cdiv(warps, nw);
   // a packet stack holds at most one pending sibling per level, plus the roots
   int stack_len = std::max(kStack, t->depth + 4 + (qroot ? 32 : 0));
+  Scratch sc(s);
   int32_t* gstack = nullptr;
   if (stack_len > kStack)
-    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw, s));
+    CKD_CUDA(sc.alloc(&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw));
   double r2 = r * r;  // radius**2 (cosmokdtree.f90:1112)
   if (fill) {
     // heavy rows: a warp per query; light rows: the per-lane kernel over a list
     int32_t *heavy = nullptr, *light = nullptr, *hstack = nullptr;
     unsigned* cnt = nullptr;
-    CKD_CUDA(dev_alloc((void**)&heavy, sizeof(int32_t) * nq, s));
-    CKD_CUDA(dev_alloc((void**)&light, sizeof(int32_t) * nq, s));
-    CKD_CUDA(dev_alloc((void**)&cnt, 2 * sizeof(unsigned), s));
+    CKD_CUDA(sc.alloc(&heavy, sizeof(int32_t) * nq));
+    CKD_CUDA(sc.alloc(&light, sizeof(int32_t) * nq));
+    CKD_CUDA(sc.alloc(&cnt, 2 * sizeof(unsigned)));
     CKD_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s));
     k_split_rows<<<(unsigned)cdiv(nq, 256), 256, 0, s>>>(offsets, order, nq, heavy, cnt, light,
                                                          cnt + 1);
@@ -805,11 +806,11 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     const int64_t hblocks = std::min<int64_t>(cdiv(nq, 4), (int64_t)sms * 8);
     const int hstack_len = std::max(kHeavyStack, t->depth + 4);
     if (hstack_len > kHeavyStack)
-      CKD_CUDA(dev_alloc((void**)&hstack, sizeof(int32_t) * hstack_len * hblocks * 4, s));
+      CKD_CUDA(sc.alloc(&hstack, sizeof(int32_t) * hstack_len * hblocks * 4));
     EmitTask* tasks = nullptr;
     unsigned* ntask = nullptr;
-    CKD_CUDA(dev_alloc((void**)&tasks, sizeof(EmitTask) * kTaskCap, s));
-    CKD_CUDA(dev_alloc((void**)&ntask, sizeof(unsigned), s));
+    CKD_CUDA(sc.alloc(&tasks, sizeof(EmitTask) * kTaskCap));
+    CKD_CUDA(sc.alloc(&ntask, sizeof(unsigned)));
     CKD_CUDA(cudaMemsetAsync(ntask, 0, sizeof(unsigned), s));
     k_ball_fill_warp<D, PER><<<(unsigned)std::max<int64_t>(1, hblocks), 128, 0, s>>>(
         tv, q, heavy, cnt, r2, hstack, hstack_len, offsets, idx, dist, sorted ? 1 : 0, tasks,
@@ -818,9 +819,6 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     k_ball_emit<D, PER><<<(unsigned)sms * 8, 128, 0, s>>>(tv, q, tasks, ntask, idx, dist,
                                                           sorted ? 1 : 0);
     CKD_LAUNCH_CHECK();
-    for (void* p : {(void*)heavy, (void*)light, (void*)cnt, (void*)hstack, (void*)tasks,
-                    (void*)ntask})
-      dev_free(p, s);
   } else {
     if (qroot)
       k_ball<D, PER, false, true><<<blocks, threads, 0, s>>>(tv, q, order, nq, nullptr, r2,
@@ -836,9 +834,9 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
     int32_t* big = nullptr;
     int64_t* toff = nullptr;
     unsigned long long* sel = nullptr;
-    CKD_CUDA(dev_alloc((void**)&big, sizeof(int32_t) * nq, s));
-    CKD_CUDA(dev_alloc((void**)&toff, sizeof(int64_t) * nq, s));
-    CKD_CUDA(dev_alloc((void**)&sel, 2 * sizeof(unsigned long long), s));
+    CKD_CUDA(sc.alloc(&big, sizeof(int32_t) * nq));
+    CKD_CUDA(sc.alloc(&toff, sizeof(int64_t) * nq));
+    CKD_CUDA(sc.alloc(&sel, 2 * sizeof(unsigned long long)));
     CKD_CUDA(cudaMemsetAsync(sel, 0, 2 * sizeof(unsigned long long), s));
     k_sort_rows<<<(unsigned)cdiv(nq, 128), 128, 0, s>>>(offsets, nq, idx, dist, big, sel, toff);
     CKD_LAUNCH_CHECK();
@@ -849,8 +847,8 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
       int64_t* tidx = nullptr;
       double* tdist = nullptr;
       if (hs[1] > 0) {
-        CKD_CUDA(dev_alloc((void**)&tidx, sizeof(int64_t) * hs[1], s));
-        CKD_CUDA(dev_alloc((void**)&tdist, sizeof(double) * hs[1], s));
+        CKD_CUDA(sc.alloc(&tidx, sizeof(int64_t) * hs[1]));
+        CKD_CUDA(sc.alloc(&tdist, sizeof(double) * hs[1]));
       }
       int dev = 0, sms = 148;
       CKD_CUDA(cudaGetDevice(&dev));
@@ -858,12 +856,8 @@ ckd_status ball_launch(const ckd_tree* t, const double* q, const int32_t* order,
       const unsigned g = (unsigned)std::min<unsigned long long>(hs[0], (unsigned long long)sms * 8);
       k_sort_big<<<g, 256, 0, s>>>(offsets, big, sel, toff, idx, dist, tidx, tdist);
       CKD_LAUNCH_CHECK();
-      dev_free(tidx, s);
-      dev_free(tdist, s);
     }
-    for (void* p : {(void*)big, (void*)toff, (void*)sel}) dev_free(p, s);
   }
-  if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
 }
 
@@ -895,9 +889,10 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
   unsigned blocks = (unsigned)cdiv(warps, nw);
   // a packet stack grows by at most one entry per level past its start entries
   int stack_len = std::max(kStack, t->depth + 4 + (broot ? 32 : 0));
+  Scratch sc(s);
   int32_t* gstack = nullptr;
   if (stack_len > kStack)
-    CKD_CUDA(dev_alloc((void**)&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw, s));
+    CKD_CUDA(sc.alloc(&gstack, sizeof(int32_t) * 2 * stack_len * (int64_t)blocks * nw));
   if (fill)
     k_box<D, true><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, nullptr, offsets,
                                               idx, broot);
@@ -905,7 +900,6 @@ ckd_status box_launch(const ckd_tree* t, const double* boxes, int64_t nb, bool f
     k_box<D, false><<<blocks, threads, 0, s>>>(tv, boxes, nb, gstack, stack_len, counts, nullptr,
                                                nullptr, broot);
   CKD_LAUNCH_CHECK();
-  if (gstack) CKD_CUDA(dev_free(gstack, s));
   return CKD_OK;
 }
 
@@ -919,8 +913,9 @@ ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bo
                     int64_t* counts, const int64_t* offsets, int64_t* idx, double* dist,
                     cudaStream_t s, const int32_t* qroot) {
   int32_t* order = nullptr;
+  Scratch sc(s);
   if (want_order(t, nq)) {
-    CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
+    CKD_CUDA(sc.alloc(&order, sizeof(int32_t) * nq));
     CKD_TRY(query_order_roots(t, q, nq, order, qroot, s));
   }
   ckd_status st;
@@ -943,7 +938,6 @@ ckd_status ball_run(const ckd_tree* t, const double* q, int64_t nq, double r, bo
     default: st = fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
   }
 #undef CKD_BALL_CASE
-  if (order) dev_free(order, s);
   return st;
 }
 

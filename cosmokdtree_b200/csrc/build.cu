@@ -964,8 +964,9 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   // trees of a forest: positions off[t] .. off[t+1]-1, root node t
   const int32_t T = (int32_t)t->n_trees;
   const std::vector<int64_t>& off = t->tree_off;
+  Scratch sc(s);  // small per-build buffers (tree offsets, box sides)
   int64_t* off_dev = nullptr;
-  CKD_CUDA(dev_alloc((void**)&off_dev, sizeof(int64_t) * (T + 1), s));
+  CKD_CUDA(sc.alloc(&off_dev, sizeof(int64_t) * (T + 1)));
   CKD_CUDA(cudaMemcpyAsync(off_dev, off.data(), sizeof(int64_t) * (T + 1), cudaMemcpyHostToDevice, s));
   {
     unsigned g = (unsigned)cdiv(n, 256);
@@ -979,7 +980,7 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     CKD_LAUNCH_CHECK();
   }
   double* Ldev = nullptr;
-  CKD_CUDA(dev_alloc((void**)&Ldev, sizeof(double) * CKD_MAX_D, s));
+  CKD_CUDA(sc.alloc(&Ldev, sizeof(double) * CKD_MAX_D));
   CKD_CUDA(cudaMemcpyAsync(Ldev, t->L, sizeof(double) * CKD_MAX_D, cudaMemcpyHostToDevice, s));
   CKD_TRY(ensure_node_cap(B, (int64_t)T + std::max<int64_t>(64, 4 * (n / std::max(1, leaf)) + 64), s));
   k_root_init<D><<<(unsigned)cdiv(T, 128), 128, 0, s>>>(B.meta, B.cell, B.keys, off_dev, T, Ldev,
@@ -1009,16 +1010,10 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
         return x;
       };
       double lo = inv(rk[(size_t)tr * 2 * D + 2 * j]), hi = inv(rk[(size_t)tr * 2 * D + 2 * j + 1]);
-      if (!std::isfinite(lo) || !std::isfinite(hi)) {
-        dev_free(Ldev, s);
-        dev_free(off_dev, s);
+      if (!std::isfinite(lo) || !std::isfinite(hi))
         return fail(CKD_ERR_BAD_ARG, "points contain NaN or infinite coordinates");
-      }
-      if (t->periodic && (lo < -t->L[j] / 2 || hi > t->L[j] / 2)) {
-        dev_free(Ldev, s);
-        dev_free(off_dev, s);
+      if (t->periodic && (lo < -t->L[j] / 2 || hi > t->L[j] / 2))
         return fail(CKD_ERR_OUT_OF_BOX, "Points outside (-L/2, L/2) range");
-      }
       rlo[j] = std::min(rlo[j], lo);
       rhi[j] = std::max(rhi[j], hi);
     }
@@ -1054,7 +1049,6 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
     CKD_CUDA(cudaMemcpyAsync(B.act[0], roots.data(), sizeof(int32_t) * roots.size(),
                              cudaMemcpyHostToDevice, s));
   CKD_CUDA(cudaStreamSynchronize(s));  // `roots`, `wst0` and `rk` are host buffers of the copies
-  dev_free(off_dev, s);
 
   // the staged scatter needs 16-byte aligned rows (even stride) and fits D <= 4
   // (<= 72 KB of shared memory per block)
@@ -1081,10 +1075,8 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   int alist = 0;  // open list buffer of the next level
   int level = 0;  // levels launched
   while (m > 0) {
-    if (level >= kMaxLevels) {
-      dev_free(Ldev, s);
+    if (level >= kMaxLevels)
       return fail(CKD_ERR_DEPTH, "tree depth exceeds the build's level cap (8192 levels)");
-    }
     int64_t mb[kRunAhead];
     mb[0] = m;
     int64_t grow = 2 * m;
@@ -1145,7 +1137,6 @@ ckd_status build_impl(ckd_tree* t, const void* pts_dev, int dtype, cudaStream_t 
   }
   int32_t err = 0;
   CKD_CUDA(cudaMemcpyAsync(&err, B.scal + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  dev_free(Ldev, s);
 
   k_leaf_box<D><<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(B.meta, n_nodes, leaf, t->pts, n,
                                                              B.box);

@@ -10,6 +10,23 @@
 
 #define CKD_MAX_D 8
 
+// Loads of tree records in the search helpers (ckd_traverse.cuh, ckd_knn.cuh,
+// ckd_knn_lane.cuh).  By default they take the read-only path (__ldg): the tree
+// does not change during a launch.  A translation unit whose kernel reads tree
+// records written earlier in the same launch (the persistent forest kernel)
+// defines CKD_TREE_LOADS_L2 before including these headers: its loads then go
+// to L2 (__ldcg), because an SM's L1 is not coherent with other SMs' stores.
+// The helpers live in an inline namespace named after the policy, so the two
+// compiled forms never share a symbol.
+#ifdef CKD_TREE_LOADS_L2
+#define CKD_LDT(p) __ldcg(p)
+#define CKD_LD_BEGIN inline namespace loads_l2 {
+#else
+#define CKD_LDT(p) __ldg(p)
+#define CKD_LD_BEGIN inline namespace loads_nc {
+#endif
+#define CKD_LD_END }
+
 namespace ckd {
 
 // ---------------------------------------------------------------- errors
@@ -59,6 +76,34 @@ void timing_end(cudaStream_t s);
 // stream-ordered scratch allocation from a per-device pool
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t dev_free(void* p, cudaStream_t s);
+
+// The pool buffers of one call: each joins the guard when it is allocated and
+// returns to the pool (in stream order) when the guard goes out of scope, on the
+// error paths too.
+struct Scratch {
+  cudaStream_t s;
+  std::vector<void*> ps;
+  explicit Scratch(cudaStream_t st) : s(st) {}
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+  ~Scratch() {
+    for (void* p : ps) dev_free(p, s);
+  }
+  template <typename T>
+  cudaError_t alloc(T** p, size_t bytes) {
+    const cudaError_t e = dev_alloc(reinterpret_cast<void**>(p), bytes, s);
+    if (e == cudaSuccess)
+      ps.push_back(*p);
+    else
+      *p = nullptr;
+    return e;
+  }
+  // hand a buffer to the caller instead of freeing it
+  void release(const void* p) {
+    for (auto& x : ps)
+      if (x == p) x = nullptr;
+  }
+};
 
 // ------------------------------------------------------------- node layout
 // One 32-byte record per node.  Children of an internal node are allocated as a

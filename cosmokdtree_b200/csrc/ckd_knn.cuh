@@ -8,6 +8,8 @@
 
 namespace ckd {
 
+CKD_LD_BEGIN
+
 constexpr int kSmemK = 64;        // largest k whose heaps live in shared memory
 constexpr int kLaneStack = 128;   // per-lane traversal stack of k_knn_lane2
 
@@ -31,7 +33,7 @@ __device__ __forceinline__ float node_mind_lb(const TreeView& tv, const QueryScr
   float s = 0.0f;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    float2 lh = __ldg(reinterpret_cast<const float2*>(b) + j);
+    float2 lh = CKD_LDT(reinterpret_cast<const float2*>(b) + j);
     float x = qs.q32[j], g;
     if (x >= lh.x - qs.dlt[j] && x <= lh.y + qs.dlt[j]) {
       g = 0.0f;
@@ -116,7 +118,7 @@ struct CompactCtx {
     return p >= 0 ? point_d2_rec<D, PER>(tv, q, p) : (p == kPosMissing ? CKD_HUGE : rr);
   }
   __device__ __forceinline__ int32_t id(int32_t p) const {
-    return p >= 0 ? __ldg(&tv.ids[p]) : (p == kPosMissing ? -1 : 0x7fffffff);
+    return p >= 0 ? CKD_LDT(&tv.ids[p]) : (p == kPosMissing ? -1 : 0x7fffffff);
   }
   // exact (d2, id) order of two entries whose FP32 keys are equal
   __device__ __forceinline__ bool tie_before(const double (&q)[D], int32_t a, int32_t b) const {
@@ -157,7 +159,7 @@ __device__ __forceinline__ bool compact_offer(CompactHeap& h, int k, const Compa
   if (kc == h.wk) {  // FP32 tie with the root: exact comparison
     const double dr = cx.exact(q, h.wp);
     if (d2 > dr) return false;
-    if (d2 == dr && __ldg(&cx.tv.ids[p]) >= cx.id(h.wp)) return false;
+    if (d2 == dr && CKD_LDT(&cx.tv.ids[p]) >= cx.id(h.wp)) return false;
   }
   uint2* H = h.H;
   int s = 1;
@@ -179,7 +181,7 @@ __device__ __forceinline__ bool compact_offer(CompactHeap& h, int k, const Compa
     bool cand_before = kc < kch;
     if (kc == kch) {
       const double dch = cx.exact(q, pch);
-      cand_before = d2 < dch || (d2 == dch && __ldg(&cx.tv.ids[p]) < cx.id(pch));
+      cand_before = d2 < dch || (d2 == dch && CKD_LDT(&cx.tv.ids[p]) < cx.id(pch));
     }
     if (!cand_before) break;
     H[s * 32] = ch;
@@ -247,13 +249,15 @@ __device__ __forceinline__ void compact_write(const TreeView& tv, const uint2* H
       int64_t id = -2;
       if (p >= 0) {
         d2 = point_d2_rec<D, PER>(tv, qx, p);
-        id = (int64_t)__ldg(&tv.ids[p]);
+        id = (int64_t)CKD_LDT(&tv.ids[p]);
       }
       dist[row * k + j] = sqrt(d2);
       idx[row * k + j] = id;
     }
   }
 }
+
+CKD_LD_END
 
 // The warp-converged kNN kernel (knn_warp.cu).  Returns false without launching
 // when the tree or k is outside its limits (the caller then uses another kernel).

@@ -6,6 +6,8 @@
 
 namespace ckd {
 
+CKD_LD_BEGIN
+
 // Squared distance between the lane's query and leaf-ordered point p
 // (cosmokdtree.f90:1441-1465: dx = p - q, minimum image, d2 = sum dx^2 in axis order).
 template <int D, bool PER>
@@ -13,7 +15,7 @@ __device__ __forceinline__ double point_d2(const TreeView& tv, const double (&q)
   double s = 0.0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    double dx = dsub(__ldg(&tv.pts[(int64_t)j * tv.n + p]), q[j]);
+    double dx = dsub(CKD_LDT(&tv.pts[(int64_t)j * tv.n + p]), q[j]);
     if (PER) dx = min_image(dx, tv.L[j]);
     s = (j == 0) ? dmul(dx, dx) : dadd(s, dmul(dx, dx));
   }
@@ -28,7 +30,7 @@ __device__ __forceinline__ double point_d2_rec(const TreeView& tv, const double 
 #pragma unroll
   for (int h = 0; h < NV; ++h) {
     const double2* r = reinterpret_cast<const double2*>(tv.pts64 + (int64_t)p * NV + h);
-    const double2 a = __ldg(r), b = __ldg(r + 1);
+    const double2 a = CKD_LDT(r), b = CKD_LDT(r + 1);
     v[4 * h] = a.x;
     v[4 * h + 1] = a.y;
     v[4 * h + 2] = b.x;
@@ -52,7 +54,7 @@ __device__ __forceinline__ double box_mind2(const TreeView& tv, const double (&q
   double s = 0.0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    double g = axis_gap<PER>(q[j], __ldg(&b[2 * j]), __ldg(&b[2 * j + 1]), tv.L[j]);
+    double g = axis_gap<PER>(q[j], CKD_LDT(&b[2 * j]), CKD_LDT(&b[2 * j + 1]), tv.L[j]);
     s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
   }
   return s;
@@ -66,8 +68,8 @@ __device__ __forceinline__ double box_maxd2(const TreeView& tv, const double (&q
   double s = 0.0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    double a = fabs(dsub(q[j], __ldg(&b[2 * j])));
-    double c = fabs(dsub(q[j], __ldg(&b[2 * j + 1])));
+    double a = fabs(dsub(q[j], CKD_LDT(&b[2 * j])));
+    double c = fabs(dsub(q[j], CKD_LDT(&b[2 * j + 1])));
     double g = a > c ? a : c;
     s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
   }
@@ -87,8 +89,8 @@ __device__ __forceinline__ double box_maxd2_near(const TreeView& tv, const doubl
   double s = 0.0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    double a = fabs(dsub(q[j], __ldg(&b[2 * j])));
-    double c = fabs(dsub(q[j], __ldg(&b[2 * j + 1])));
+    double a = fabs(dsub(q[j], CKD_LDT(&b[2 * j])));
+    double c = fabs(dsub(q[j], CKD_LDT(&b[2 * j + 1])));
     double g = a > c ? a : c;
     if (!(g <= 0.5 * tv.L[j])) return CUDART_INF;
     s = (j == 0) ? dmul(g, g) : dadd(s, dmul(g, g));
@@ -98,7 +100,7 @@ __device__ __forceinline__ double box_maxd2_near(const TreeView& tv, const doubl
 
 __device__ __forceinline__ NodeMeta load_meta(const NodeMeta* m, int32_t node) {
   const int4* p = reinterpret_cast<const int4*>(m + node);
-  int4 a = __ldg(p), b = __ldg(p + 1);
+  int4 a = CKD_LDT(p), b = CKD_LDT(p + 1);
   NodeMeta r;
   r.split = __hiloint2double(a.y, a.x);
   r.left = a.z;
@@ -109,6 +111,8 @@ __device__ __forceinline__ NodeMeta load_meta(const NodeMeta* m, int32_t node) {
   r.parent = b.w;
   return r;
 }
+
+CKD_LD_END
 
 // Order queries by the leaf they fall in (a counting sort on the leaf's first
 // point), so that the 32 lanes of a warp hold spatially adjacent queries.

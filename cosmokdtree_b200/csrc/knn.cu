@@ -1,7 +1,6 @@
 // knn.cu -- exact k-nearest-neighbour search (cosmokdtree.f90:504-905): query
 // ordering, the per-lane and packet kernels, the kernel choice, forests, the
-// learned-bound path and the allocation-free entry point.  The default kernel
-// for leaf-ordered queries is the warp-converged one in knn_warp.cu.
+// learned-bound path and the allocation-free entry point.
 //
 // One query per lane.  Each lane keeps its k best (squared distance, id) in a
 // max-heap (root = current k-th); a candidate enters iff it ranks strictly before
@@ -14,6 +13,7 @@
 
 #include "ckd_common.cuh"
 #include "ckd_knn.cuh"
+#include "ckd_knn_lane.cuh"
 #include "ckd_mlp.cuh"
 #include "ckd_scan.cuh"
 #include "ckd_traverse.cuh"
@@ -253,22 +253,7 @@ __global__ void __launch_bounds__(128) k_knn_rows(TreeView tv, const double* __r
   }
 }
 
-// ====================================== per-lane traversal, compact heap
-// Each lane walks the tree for its own query: both children's FP32 boxes are
-// tested when a node is expanded, the nearer child is taken and the other pushed
-// with its bound on a per-lane stack, so entries that the shrinking k-th distance
-// has pruned are dropped without reloading a node.  Lanes descend until they
-// reach a leaf, then scan leaves together (while-while structure): an FP32 screen
-// on leaf-relative coordinates, an FP64 recheck and the compact heap.  Used for
-// unordered query batches, for the learned path's reruns, by the allocation-free
-// entry point and as the learned path's bounded kernel when selected.
-//
-// BOUNDED: every query starts with its heap full of k sentinels (key r2[q],
-// id INT32_MAX) instead of HUGE, so pruning starts at the root.  A point is
-// accepted iff (d2, id) < the current worst, so every point with d2 <= r2[q] is
-// still seen; when no sentinel is left the heap holds the exact k nearest.  A
-// query that ends with a sentinel (fewer than k points within the bound) is
-// appended to miss[] for the unbounded rerun and its output row is not written.
+// The per-lane kernel: one warp per 32 query slots (knn_lane_run).
 template <int D, bool PER, bool BOUNDED = false, bool PAIR = false>
 __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double* __restrict__ Q,
                                                    const int32_t* __restrict__ order, int64_t nq,
@@ -280,295 +265,12 @@ __global__ void __launch_bounds__(128, 6) k_knn_lane2(TreeView tv, const double*
                                                    unsigned* __restrict__ nmiss = nullptr,
                                                    const int32_t* __restrict__ qleaf = nullptr,
                                                    const int32_t* __restrict__ qroot = nullptr) {
-  constexpr int NV = (D + 3) / 4;
-  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // heap slot s of this lane at H[s * 32 + lane]: (key bits, position); keys are
-  // non-negative floats, so their bit patterns order as unsigned integers, and
-  // every lane always addresses its own bank pair (no conflicts between lanes
-  // at different heap levels)
-  uint2* H = reinterpret_cast<uint2*>(smem) + (size_t)w * 32 * (k + 1) + lane;
+  uint2* Hw = reinterpret_cast<uint2*>(smem) + (size_t)w * 32 * (k + 1);
   const int64_t gw = (int64_t)blockIdx.x * nw + w;
-  const int64_t slot = gw * 32 + lane;
-  const bool valid = slot < nq;
-  const int64_t qi = valid ? (order ? (int64_t)order[slot] : slot) : 0;
-  double q[D];
-  QueryScreen<D, PER> qs;
-#pragma unroll
-  for (int j = 0; j < D; ++j) {
-    q[j] = valid ? Q[qi * D + j] : 0.0;
-    qs.q32[j] = __double2float_rn(q[j]);
-    qs.dlt[j] = kTwoM21 * (fabsf(qs.q32[j]) + tv.slack[j]) * 1.0001f;
-  }
-  float skey = FLT_MAX;
-  int32_t spos = kPosMissing;
-  float wd32 = FLT_MAX;
-  double rr = CKD_HUGE;
-  if (BOUNDED && valid) {
-    const double b = r2[qi];
-    if (b < CKD_HUGE) {
-      rr = b;
-      skey = __double2float_rn(b);
-      spos = kPosBound;
-      wd32 = __double2float_ru(b);
-    }
-  }
-  const CompactCtx<D, PER> cx{tv, rr};
-  CompactHeap hp{H, 0u, 0, 0.0f};
-  compact_init<D, PER>(hp, k, skey, spos, wd32);
-  // Direct box gaps max(lo - xl, xh - hi, 0) while the query's ball cannot reach
-  // the periodic box faces (wf: then the closest image of any point that can
-  // still enter the heap is the point itself), and point screens on absolute
-  // FP32 coordinates with the per-query error bounds Ed (direct) / Ew (minimum
-  // image): fl32(fl32(p_j) - fl32(q_j)) is within 2^-23 (B_j + |q_j|) of
-  // p_j - q_j, so e_j = 2^-22 (B_j + |q_j|) bounds it with a factor-2 margin and
-  // a point whose FP64 squared distance is <= tau has an FP32 sum of squares
-  // <= (sqrt(tau) + |e|)^2 / (1 - 2^-20).
-  float xl[D], xh[D], Ed = 0.0f, Ew = 0.0f;
-  bool wf = !PER;
-  {
-    float e2 = 0.0f, e2w = 0.0f;
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-      xl[j] = __fadd_ru(qs.q32[j], qs.dlt[j]);
-      xh[j] = __fsub_rd(qs.q32[j], qs.dlt[j]);
-      const float ej = __fmaf_ru(kTwoM22, __fadd_ru(tv.slack[j], fabsf(qs.q32[j])), 1e-37f);
-      e2 = __fmaf_ru(ej, ej, e2);
-      const float ejw = PER ? __fmaf_ru(kTwoM22, (float)tv.L[j], ej) : ej;
-      e2w = __fmaf_ru(ejw, ejw, e2w);
-    }
-    Ed = sqrt_up(e2);
-    Ew = sqrt_up(e2w);
-  }
-  auto box_lb = [&](const float* lo, const float* hi) -> float {
-    if (!PER || wf) {
-      float s2 = 0.0f;
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        const float g = fmaxf(fmaxf(lo[j] - xl[j], xh[j] - hi[j]), 0.0f);
-        s2 = fmaf(g, g, s2);
-      }
-      return s2 * kShrink;
-    }
-    float lo4[4 * NV], hi4[4 * NV];
-#pragma unroll
-    for (int j = 0; j < 4 * NV; ++j) {
-      lo4[j] = j < D ? lo[j] : 0.0f;
-      hi4[j] = j < D ? hi[j] : 0.0f;
-    }
-    return box_mind_lb<D, PER>(tv, qs, lo4, hi4);
-  };
-  auto node_lb = [&](int32_t nd) -> float {
-    float lo[D], hi[D];
-    const float2* b = reinterpret_cast<const float2*>(tv.box32 + (int64_t)nd * 2 * D);
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-      const float2 lh = __ldg(b + j);
-      lo[j] = lh.x;
-      hi[j] = lh.y;
-    }
-    return box_lb(lo, hi);
-  };
-
-  int32_t sn[kLaneStack];
-  float sd[kLaneStack];
-  int top = 0;
-  int32_t node = valid ? (qroot ? qroot[qi] : 0) : -1;
-  if (BOUNDED && valid && qleaf && spos == kPosBound) {
-    // start at the lowest ancestor whose cell strictly contains [q - r, q + r]^D
-    const float r32 = __fsqrt_ru(hp.wd32);
-    int32_t a = qleaf[qi];
-    while (a >= 0) {
-      const float* c = tv.cell32 + (int64_t)a * 2 * D;
-      bool inside = true;
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        const float2 lh = __ldg(reinterpret_cast<const float2*>(c) + j);
-        inside = inside && __fsub_rd(__fsub_rd(qs.q32[j], r32), qs.dlt[j]) > lh.x &&
-                 __fadd_ru(__fadd_ru(qs.q32[j], r32), qs.dlt[j]) < lh.y;
-      }
-      if (inside) break;
-      a = load_meta(tv.meta, a).parent;
-    }
-    node = a < 0 ? node : a;
-  }
-  // PAIR: stack entries and `node` carry the leaf flag (a leaf is stored as ~id,
-  // < -1 because children ids are >= 1; -1 means "no node") and internal nodes are
-  // expanded from their child-pair record alone (both children's FP32 boxes, ids
-  // and leaf flags), one dependent load per level.  Otherwise the node's meta is
-  // read first, then both children's FP32 boxes.
-  constexpr int PF = pair_f4(D);
-  bool is_leaf = node >= 0 && PAIR && load_meta(tv.meta, node).left < 0;
-  NodeMeta m;
-  while (node >= 0) {
-    // ---- descend to a leaf, nearer child first
-    if (!PAIR) {
-      m = load_meta(tv.meta, node);
-      while (node >= 0 && m.left >= 0) {
-        if (stats) st[0] += 1;
-        const float ml = node_lb(m.left);
-        const float mr = node_lb(m.left + 1);
-        const bool nl = ml <= hp.wd32, nr = mr <= hp.wd32;
-        if (nl && nr) {
-          const bool lf = ml <= mr;
-          sn[top] = lf ? m.left + 1 : m.left;
-          sd[top] = lf ? mr : ml;
-          ++top;
-          node = lf ? m.left : m.left + 1;
-        } else if (nl || nr) {
-          node = nl ? m.left : m.left + 1;
-        } else {
-          node = -1;
-          while (top > 0) {
-            --top;
-            if (sd[top] <= hp.wd32) {
-              node = sn[top];
-              break;
-            }
-          }
-        }
-        if (node >= 0) m = load_meta(tv.meta, node);
-      }
-      if (node < 0) break;
-    } else {
-      while (!is_leaf) {
-        if (stats) st[0] += 1;
-        const float4* rec = tv.pair + (int64_t)node * PF;
-        float lo_l[4 * NV], hi_l[4 * NV], lo_r[4 * NV], hi_r[4 * NV];
-#pragma unroll
-        for (int h = 0; h < NV; ++h) {
-          const float4 a = __ldg(rec + h), b = __ldg(rec + NV + h);
-          const float4 c = __ldg(rec + 2 * NV + h), d = __ldg(rec + 3 * NV + h);
-          lo_l[4 * h] = a.x; lo_l[4 * h + 1] = a.y; lo_l[4 * h + 2] = a.z; lo_l[4 * h + 3] = a.w;
-          hi_l[4 * h] = b.x; hi_l[4 * h + 1] = b.y; hi_l[4 * h + 2] = b.z; hi_l[4 * h + 3] = b.w;
-          lo_r[4 * h] = c.x; lo_r[4 * h + 1] = c.y; lo_r[4 * h + 2] = c.z; lo_r[4 * h + 3] = c.w;
-          hi_r[4 * h] = d.x; hi_r[4 * h + 1] = d.y; hi_r[4 * h + 2] = d.z; hi_r[4 * h + 3] = d.w;
-        }
-        const int4 info = __ldg(reinterpret_cast<const int4*>(rec + 4 * NV));
-        const float ml = box_lb(lo_l, hi_l);
-        const float mr = box_lb(lo_r, hi_r);
-        const bool nl = ml <= hp.wd32, nr = mr <= hp.wd32;
-        const int32_t el = info.z ? ~info.x : info.x, er = info.w ? ~info.y : info.y;
-        int32_t nxt = -1;
-        if (nl && nr) {
-          const bool lf = ml <= mr;
-          sn[top] = lf ? er : el;
-          sd[top] = lf ? mr : ml;
-          ++top;
-          nxt = lf ? el : er;
-        } else if (nl || nr) {
-          nxt = nl ? el : er;
-        } else {
-          while (top > 0) {
-            --top;
-            if (sd[top] <= hp.wd32) {
-              nxt = sn[top];
-              break;
-            }
-          }
-          if (nxt == -1) break;
-        }
-        is_leaf = nxt < 0;
-        node = is_leaf ? ~nxt : nxt;
-      }
-      if (!is_leaf) break;
-      m = load_meta(tv.meta, node);
-    }
-
-    // ---- scan the leaf
-    if (stats) {
-      st[2] += 1;
-      st[3] += m.count;
-    }
-    {
-      if (PER && !wf) {
-        const float r32 = sqrt_up(hp.wd32);
-        bool inside = true;
-#pragma unroll
-        for (int j = 0; j < D; ++j)
-          inside = inside && __fadd_ru(__fadd_ru(fabsf(qs.q32[j]), r32), qs.dlt[j]) <
-                                 0.5f * (float)tv.L[j];
-        wf = inside;
-      }
-      for (int base = 0; base < m.count; base += 32) {
-        const int cnt = min(32, m.count - base);
-        const int32_t p0 = m.start + base;
-        const float t = __fadd_ru(sqrt_up(hp.wd32), wf ? Ed : Ew);
-        const float thr = __fmul_ru(__fmul_ru(t, t), 1.0000020f);
-        unsigned mask = 0;
-        for (int i = 0; i < cnt; ++i) {
-          float v[4 * NV];
-#pragma unroll
-          for (int h = 0; h < NV; ++h) {
-            const float4 f = __ldg(&tv.pts32[(int64_t)(p0 + i) * NV + h]);
-            v[4 * h] = f.x;
-            v[4 * h + 1] = f.y;
-            v[4 * h + 2] = f.z;
-            v[4 * h + 3] = f.w;
-          }
-          float s2 = 0.0f;
-#pragma unroll
-          for (int j = 0; j < D; ++j) {
-            float a = v[j] - qs.q32[j];
-            if (PER && !wf) {
-              a = fabsf(a);
-              a = fminf(a, (float)tv.L[j] - a);
-            }
-            s2 = fmaf(a, a, s2);
-          }
-          if (s2 <= thr) mask |= 1u << i;
-        }
-        if (stats) st[5] += __popc(mask);
-        while (mask) {
-          const int i = __ffs(mask) - 1;
-          mask &= mask - 1;
-          const int32_t p = p0 + i;
-          const double d2 = point_d2_rec<D, PER>(tv, q, p);
-          if (compact_offer<D, PER>(hp, k, cx, q, d2, p) && stats) st[6] += 1;
-        }
-      }
-    }
-    // ---- next: pop the nearest pending subtree still within reach
-    int32_t nxt = -1;
-    while (top > 0) {
-      --top;
-      if (sd[top] <= hp.wd32) {
-        nxt = sn[top];
-        break;
-      }
-    }
-    if (nxt == -1) break;
-    if (PAIR) {
-      is_leaf = nxt < 0;
-      node = is_leaf ? ~nxt : nxt;
-    } else {
-      node = nxt;
-    }
-  }
-  if (stats) {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      unsigned long long v = st[c];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-      if (lane == 0) atomicAdd(&stats[c], v);
-    }
-  }
-  const bool missed = BOUNDED && valid && hp.wp == kPosBound;
-  unsigned missmask = 0;
-  if (BOUNDED) {
-    missmask = __ballot_sync(FULL, missed);
-    if (missmask) {
-      unsigned base = 0;
-      if (lane == 0) base = atomicAdd(nmiss, (unsigned)__popc(missmask));
-      base = __shfl_sync(FULL, base, 0);
-      if (missed) miss[base + __popc(missmask & ((1u << lane) - 1u))] = (int32_t)qi;
-    }
-  }
-  if (sorted && valid && !missed) compact_sort<D, PER>(hp.H, k, cx, q);
-  __syncwarp();
-  compact_write<D, PER>(tv, hp.H - lane, lane, gw, nq, order, q, k, missmask, dist, idx);
+  knn_lane_run<D, PER, BOUNDED, PAIR>(tv, Q, order, nq, k, sorted, dist, idx, stats, r2, miss,
+                                      nmiss, qleaf, qroot, 0, Hw, lane, gw);
 }
 // ------------------------------------------------------------ query order
 template <int D>
@@ -691,10 +393,11 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
                       int32_t* qleaf, cudaStream_t s, int32_t** off_out = nullptr,
                       const int32_t* qroot = nullptr) {
   int64_t n = t->n;
+  Scratch sc(s);
   int32_t *key = nullptr, *hist = nullptr, *off = nullptr;
-  CKD_CUDA(dev_alloc((void**)&key, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&hist, sizeof(int32_t) * n, s));
-  CKD_CUDA(dev_alloc((void**)&off, sizeof(int32_t) * (n + 1), s));
+  CKD_CUDA(sc.alloc(&key, sizeof(int32_t) * nq));
+  CKD_CUDA(sc.alloc(&hist, sizeof(int32_t) * n));
+  CKD_CUDA(sc.alloc(&off, sizeof(int32_t) * (n + 1)));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   unsigned g = (unsigned)cdiv(nq, 256);
   k_locate<D><<<g, 256, 0, s>>>(t->meta, q, nq, key, hist, qleaf, qroot);
@@ -703,12 +406,10 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * n, s));
   k_bucket_scatter<<<g, 256, 0, s>>>(key, nq, off, hist, order);
   CKD_LAUNCH_CHECK();
-  CKD_CUDA(dev_free(key, s));
-  CKD_CUDA(dev_free(hist, s));
-  if (off_out)
+  if (off_out) {
     *off_out = off;
-  else
-    CKD_CUDA(dev_free(off, s));
+    sc.release(off);
+  }
   return CKD_OK;
 }
 
@@ -890,11 +591,12 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
   int32_t *order = nullptr, *qleaf = nullptr, *miss = nullptr;
   double* r2 = nullptr;
   unsigned* nmiss = nullptr;
-  CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&qleaf, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&r2, sizeof(double) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&miss, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&nmiss, sizeof(unsigned), s));
+  Scratch sc(s);
+  CKD_CUDA(sc.alloc(&order, sizeof(int32_t) * nq));
+  CKD_CUDA(sc.alloc(&qleaf, sizeof(int32_t) * nq));
+  CKD_CUDA(sc.alloc(&r2, sizeof(double) * nq));
+  CKD_CUDA(sc.alloc(&miss, sizeof(int32_t) * nq));
+  CKD_CUDA(sc.alloc(&nmiss, sizeof(unsigned)));
   CKD_CUDA(cudaMemsetAsync(nmiss, 0, sizeof(unsigned), s));
   ckd_status st = order_impl<D>(t, q, nq, order, qleaf, s);
   if (st == CKD_OK) {
@@ -938,7 +640,6 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     st = knn_launch<D, PER>(t, q, miss, nullptr, (int64_t)nm, k, sorted, dist, idx, s, 7);
   if (st == CKD_OK) timing_end(s);
   if (nfb_out) *nfb_out = nm;
-  for (void* p : {(void*)order, (void*)qleaf, (void*)r2, (void*)miss, (void*)nmiss}) dev_free(p, s);
   return st;
 }
 
@@ -976,8 +677,10 @@ ckd_status knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, i
 // streams, or two host threads) race on it and must be serialised by the
 // caller.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call
-// before any stream capture.  The array holds ~18 MB on every device that
-// loads the library, until the process exits.
+// before any stream capture.  The lookup is repeated when the device's current
+// context changed since (cudaDeviceReset, a caller-made context), so such a call
+// should also come outside a capture.  The array holds ~18 MB on every device
+// that loads the library, until the process exits.
 namespace {
 
 constexpr int64_t kNoAllocMaxQ = int64_t(1) << 21;  // queries per call
@@ -989,18 +692,44 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[64] = {nullptr};
+void* g_noalloc_ctx[64] = {nullptr};
 
-// host address of the scratch array on the current device (set up once per device)
+// the driver's current context (cuCtxGetCurrent, fetched through the runtime so
+// the library needs no link against the driver library); null if unavailable
+void* current_context() {
+  using CtxFn = int (*)(void**);
+  static CtxFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxFn>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array in the current device's context, looked up
+// once per device and again whenever that device's current context is another
+// one than at the last lookup (after cudaDeviceReset, or when the caller made a
+// context of its own current): a context's module copy of the array has its own
+// address.
 ckd_status noalloc_scratch(void** out) {
   int dev = 0;
   CKD_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(CKD_ERR_NO_DEVICE, "device index out of range");
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  void* ctx = current_context();
+  if (!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
     g_noalloc_ptr[dev] = p;
+    // cudaGetSymbolAddress made the primary context current if none was
+    g_noalloc_ctx[dev] = ctx ? ctx : current_context();
   }
   *out = g_noalloc_ptr[dev];
   return CKD_OK;

@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
   const uint32_t taddr = *slot;
   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
   uint32_t phase = 0;
+  uint32_t last_commit = 0;  // parity of the last commit thread 0 issued
   bool ok = true;
 
   for (int64_t base = (int64_t)blockIdx.x * kTcRows; base < n; base += (int64_t)gridDim.x * kTcRows) {
@@ -222,6 +223,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
     if (t == 0 && ok) {
       mma_bf16(taddr, smem_desc(sA1, kTcRows, 0), smem_desc(sB1, kMlpH, 0), 0u);
       mma_commit(bar);
+      last_commit = phase;
     }
     ok = ok && bar_wait(bar, phase);
     phase ^= 1u;
@@ -245,6 +247,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
         mma_bf16(taddr + kMlpH, smem_desc(sA2, kTcRows, ks), smem_desc(sB2, kMlpH, ks),
                  ks > 0 ? 1u : 0u);
       mma_commit(bar);
+      last_commit = phase;
     }
     ok = ok && bar_wait(bar, phase);
     phase ^= 1u;
@@ -268,7 +271,14 @@ __global__ void __launch_bounds__(kTcRows, 1)
     ok = __syncthreads_and(ok);  // every lane has read D1 / D2 before the next tile's MMAs
     fence_after();
   }
-  if (!ok && t == 0) atomicExch(err, 1u);
+  // After a timed-out wait no further MMA is issued, but the one whose completion
+  // was not seen may still be writing tensor memory: thread 0 waits for it once
+  // more (bounded) before the columns are released to the next CTA.  A timeout
+  // makes every output of the launch invalid (CKD_ERR_TIMEOUT is returned).
+  if (!ok && t == 0) {
+    atomicExch(err, 1u);
+    bar_wait(bar, last_commit);
+  }
   fence_before();
   __syncthreads();
   if (warp == 0)

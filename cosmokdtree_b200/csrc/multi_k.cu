@@ -98,18 +98,25 @@ ckd_status gather_q(int d, const double* q, const int32_t* rows, int64_t n, doub
 ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* kq,
                        int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
   int32_t *hist = nullptr, *off = nullptr, *fill = nullptr, *grp = nullptr, *bad = nullptr;
-  CKD_CUDA(dev_alloc((void**)&hist, sizeof(int32_t) * (kmax + 1), s));
-  CKD_CUDA(dev_alloc((void**)&off, sizeof(int32_t) * (kmax + 2), s));
-  CKD_CUDA(dev_alloc((void**)&fill, sizeof(int32_t) * (kmax + 1), s));
-  CKD_CUDA(dev_alloc((void**)&grp, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&bad, sizeof(int32_t), s));
+  // every buffer joins the guard as soon as it exists, so a failed allocation
+  // returns the earlier ones to the pool
   struct Free {
     cudaStream_t s;
     std::vector<void*> ps;
     ~Free() {
       for (void* p : ps) dev_free(p, s);
     }
-  } fr{s, {hist, off, fill, grp, bad}};
+  } fr{s, {}};
+  auto take = [&](int32_t** p, size_t bytes) -> cudaError_t {
+    const cudaError_t e = dev_alloc((void**)p, bytes, s);
+    if (e == cudaSuccess) fr.ps.push_back(*p);
+    return e;
+  };
+  CKD_CUDA(take(&hist, sizeof(int32_t) * (kmax + 1)));
+  CKD_CUDA(take(&off, sizeof(int32_t) * (kmax + 2)));
+  CKD_CUDA(take(&fill, sizeof(int32_t) * (kmax + 1)));
+  CKD_CUDA(take(&grp, sizeof(int32_t) * nq));
+  CKD_CUDA(take(&bad, sizeof(int32_t)));
   CKD_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (kmax + 1), s));
   CKD_CUDA(cudaMemsetAsync(fill, 0, sizeof(int32_t) * (kmax + 1), s));
   CKD_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));

@@ -66,18 +66,16 @@ ckd_status scan_impl(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
     CKD_LAUNCH_CHECK();
     return CKD_OK;
   }
+  Scratch sc(s);
   Tout* part = nullptr;
   Tout* poff = nullptr;
-  CKD_CUDA(dev_alloc((void**)&part, sizeof(Tout) * tiles, s));
-  CKD_CUDA(dev_alloc((void**)&poff, sizeof(Tout) * (tiles + 1), s));
+  CKD_CUDA(sc.alloc(&part, sizeof(Tout) * tiles));
+  CKD_CUDA(sc.alloc(&poff, sizeof(Tout) * (tiles + 1)));
   k_tile_reduce<Tin, Tout><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, part);
   CKD_LAUNCH_CHECK();
-  ckd_status st = scan_impl<Tout, Tout>(part, poff, tiles, s);
-  if (st != CKD_OK) return st;
+  CKD_TRY((scan_impl<Tout, Tout>(part, poff, tiles, s)));
   k_tile_scan<Tin, Tout><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, poff, out);
   CKD_LAUNCH_CHECK();
-  CKD_CUDA(dev_free(part, s));
-  CKD_CUDA(dev_free(poff, s));
   return CKD_OK;
 }
 

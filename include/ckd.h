@@ -123,8 +123,15 @@ ckd_status ckd_set_knn_variant(int variant);
  * the learned-bound network (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on
  * BF16 activations, default); key 8: box search of up to 32768 boxes per call
  * (1 = a warp per box, frontier expanded a level at a time, default; 0 = a lane
- * per box). */
+ * per box); key 9: cap in MiB on the device memory the library's pool hands out
+ * at any time on the current device (0 = none, default): an allocation past it
+ * fails with CKD_ERR_OOM and the call returns everything it had taken. */
 ckd_status ckd_set_tuning(int key, int value);
+
+/* Bytes of the current device's library pool in use by live allocations (trees,
+ * networks, a running call's scratch) and reserved from the driver (no reference
+ * counterpart; used to check that failed calls return their scratch). */
+ckd_status ckd_pool_usage(int64_t* used, int64_t* reserved);
 
 /* Traversal statistics of the kNN kernels (diagnostics, no reference
  * counterpart).  Copies the counters accumulated since the previous call into
@@ -155,7 +162,9 @@ ckd_status ckd_kernel_ms(float* ms);
  * share the array, so calls that overlap on the GPU (other streams or threads)
  * race and must be serialised by the caller.  The first call on a device looks
  * up the array's address (cudaGetSymbolAddress); make it before any stream
- * capture. */
+ * capture.  The lookup is repeated when the device's current context has changed
+ * since (after cudaDeviceReset, or under a context the caller made current), so
+ * the first call after such a change should also come before any capture. */
 ckd_status ckd_knn_noalloc(const ckd_tree* tree, const double* q_dev, int64_t nq, int k,
                            int sorted, double* dist_dev, int64_t* idx_dev, void* stream);
 

@@ -85,3 +85,17 @@ def test_two_rank_gloo(tmp_path):
                        start_method="spawn")
     assert (tmp_path / "r0").read_text() == "ok"
     assert (tmp_path / "r1").read_text() == "ok"
+
+
+def test_bench_rejects_world_size_mismatch():
+    """bench.py --gpus N under a launcher that started another number of ranks stops
+    with an error instead of timing the wrong number of GPUs."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2"],
+                       capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 2
+    assert "WORLD_SIZE=1" in json.loads(r.stdout.strip().splitlines()[-1])["error"]

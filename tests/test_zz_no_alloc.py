@@ -20,8 +20,10 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("periodic", [False, True])
-def test_knn_noalloc_matches_knn(gpu, periodic):
+# "far": coordinates near 1e18, beyond the range where the FP32 screen is used,
+# so the entry point takes its FP64 packet kernel instead of the per-lane one
+@pytest.mark.parametrize("case", ["open", "periodic", "far"])
+def test_knn_noalloc_matches_knn(gpu, oracle, case):
     import torch
     from cosmokdtree_b200 import _lib, kdtree
     L = _lib.load()
@@ -29,11 +31,15 @@ def test_knn_noalloc_matches_knn(gpu, periodic):
     n = 60000
     P = rng.random((n, 3)) - 0.5
     P[:20000] = P[:20000] * 0.05  # a dense core
-    box = [1.0, 1.0, 1.0] if periodic else None
+    box = [1.0, 1.0, 1.0] if case == "periodic" else None
+    shift, scale = (1e18, 1e17) if case == "far" else (0.0, 1.0)
+    P = shift + scale * P
     tree = kdtree.build_kdtree(P, leaf=16, boxsize=box)
+    ot = oracle.OracleTree(P, 16, box)
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call, (nq, k) in enumerate([(20000, 32), (7000, 16)]):
-        Q = np.concatenate([P[rng.integers(0, n, nq // 2)], rng.random((nq - nq // 2, 3)) - 0.5])
+        Q = np.concatenate([P[rng.integers(0, n, nq // 2)],
+                            shift + scale * (rng.random((nq - nq // 2, 3)) - 0.5)])
         Qd = torch.from_numpy(Q).cuda()
         d_ref = torch.empty((nq, k), dtype=torch.float64, device="cuda")
         i_ref = torch.empty((nq, k), dtype=torch.int64, device="cuda")
@@ -44,6 +50,11 @@ def test_knn_noalloc_matches_knn(gpu, periodic):
         torch.cuda.synchronize()
         assert torch.equal(i_na, i_ref), f"ids differ on call {call}"
         assert torch.equal(d_na, d_ref), f"distances differ on call {call}"
+        # and both equal the CPU oracle (ids exactly, distances to the last bit)
+        sel = rng.integers(0, nq, 2000)
+        od, oi = ot.knn(Q[sel], k)
+        np.testing.assert_array_equal(i_na.cpu().numpy()[sel], oi)
+        np.testing.assert_array_equal(d_na.cpu().numpy()[sel], od)
     # the documented limit is enforced with a clear error
     big = 2097152 + 1
     st = L.ckd_knn_noalloc(tree.handle, _p(Qd), big, 8, 1, _p(d_na), _p(i_na), stream)
