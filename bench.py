@@ -252,6 +252,8 @@ def run_forest(args):
         e1.record(stream)
         torch.cuda.synchronize()
     knn_ms = e0.elapsed_time(e1) / args.steps
+    knn_i, knn_d = out[1].clone(), out[0].clone()
+    persistent = run_forest_persistent(args, Pd, off, Q, qoff, k, knn_d, knn_i, stream)
     # boxes: 64 per tree, uniform centres
     B = np.empty((n_trees * nbox, 6))
     cen = rng.random((n_trees * nbox, 3)) - 0.5
@@ -322,11 +324,59 @@ def run_forest(args):
         "boxes": {"ms": box_ms, "boxes_per_s": len(B) / (box_ms / 1e3),
                   "results": int(bo[-1].item())},
         "parity_sample": {"trees": int(len(samp)), "bit_exact": bool(ok)},
+        "persistent": persistent,
     }
     print(json.dumps(outl))
     del graph
     f.close()
     return 0
+
+
+def run_forest_persistent(args, Pd, off, Q, qoff, k, ref_d, ref_i, stream):
+    """The whole forest built and queried by ONE persistent launch over a device
+    work queue (ForestPlan), replayed as a CUDA graph: build + kNN per step.  The
+    queries per work item come from the autotuner (timed on this forest, results
+    checked equal across candidates, cached)."""
+    import torch
+    from cosmokdtree_b200 import ForestPlan
+    from cosmokdtree_b200.autotune import Autotuner
+    tuner = Autotuner()
+    cfg = tuner.tune_forest_plan(Pd, off, Q, qoff, k, boxsize=1.0, reps=2)
+    plan = ForestPlan(Pd, off, Q, qoff, k, leaf=cfg["leaf"], boxsize=1.0,
+                      queries_per_block=cfg["queries_per_block"])
+    plan.run()
+    plan.check()
+    exact = bool(torch.equal(plan.idx, ref_i) and torch.equal(plan.dist, ref_d))
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            plan.run()
+    stream.wait_stream(side)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    plan.check()
+    exact = exact and bool(torch.equal(plan.idx, ref_i) and torch.equal(plan.dist, ref_d))
+    n, nq = int(off[-1]), int(Q.shape[0])
+    pf = plan.forest()
+    out = {"method": "one persistent launch: (tree, level) build items and (tree, query "
+                     "block) kNN items on a device work queue, replayed as a CUDA graph",
+           "ms_per_step": ms, "points_per_s": n / (ms / 1e3), "queries_per_s": nq / (ms / 1e3),
+           "exact_vs_forest_knn": exact, "n_nodes": pf.n_nodes, "depth": pf.depth,
+           "tuned": {"leaf": cfg["leaf"], "queries_per_block": cfg["queries_per_block"],
+                     "key": cfg.get("key"), "candidates_ms": cfg.get("candidates_ms")}}
+    del graph
+    plan.close()
+    return out
 
 
 def run_small_uniform(args):

@@ -9,6 +9,6 @@ from .kdtree import (  # noqa: F401
     KDTree, ball_search, ball_search_csr, box_search, box_search_csr, build_kdtree,
     deallocate_kdtree, knn_search, knn_search_batch,
 )
-from .forest import Forest, build_forest  # noqa: F401
+from .forest import Forest, ForestPlan, build_forest  # noqa: F401
 
 __version__ = "0.1.0"

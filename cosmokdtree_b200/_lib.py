@@ -76,6 +76,12 @@ SIGNATURES = {
     "ckd_free": [_vp],
     "ckd_release_cached_memory": [],
     "ckd_pool_usage": [_pi64, _pi64],
+    "ckd_forest_plan_create": [_vp, _pi64, _i64, _int, _int, _pdbl, _vp, _pi64, _i64, _int, _int,
+                               _vp, _vp, _dbl, _int, ctypes.POINTER(_vp)],
+    "ckd_forest_plan_run": [_vp, _vp],
+    "ckd_forest_plan_status": [_vp, _vp],
+    "ckd_forest_plan_forest": [_vp, ctypes.POINTER(_vp)],
+    "ckd_forest_plan_free": [_vp],
     "ckd_tree_info": [_vp, _pi64, _pint, _pint, _pint, _pi32, _pi32, _pi32, _pint],
     "ckd_tree_export": [_vp, _pi32, _pdbl, _pi64, _pi64, _pi64, _pi64, _pdbl, _pdbl, _pi64],
     "ckd_knn": [_vp, _vp, _i64, _int, _int, _vp, _vp, _vp],

@@ -146,6 +146,67 @@ class Autotuner:
         return out
 
 
+    # ------------------------------------------------- persistent forest
+    def tune_forest_plan(self, points, offsets, queries, query_offsets, k: int, boxsize=None,
+                         grid: dict | None = None, reps: int = 3, key: str | None = None,
+                         save: bool = True) -> dict:
+        """Queries per work item (``queries_per_block``: 32 lanes x 4 warps per CTA
+        take 128 queries at a time, so 32..512 covers 1/4 to 4 queries per lane)
+        and leaf size of the persistent forest launch, timed as whole build + kNN
+        runs on the caller's forest; every candidate's rows must equal the first
+        candidate's bit for bit.  Cached per (d, k, periodic, forest size class,
+        GPU); returns the best config with ``key`` and ``candidates_ms``."""
+        import torch
+        from .forest import ForestPlan
+        g = {"leaf": (16,), "queries_per_block": (32, 64, 128, 256, 512)}
+        g.update(grid or {})
+        n, d = int(points.shape[0]), int(points.shape[1])
+        if key is None:
+            key = "forest-plan-" + config_key(d, int(k), "float64", boxsize is not None, n,
+                                              _device_name())
+        hit = self.cache.get(key)
+        if hit is not None:
+            out = dict(hit["config"])
+            out.update(key=key, candidates_ms=hit.get("candidates_ms"), cached=True)
+            return out
+        results, ref = [], None
+        for leaf in g["leaf"]:
+            for qb in g["queries_per_block"]:
+                plan = ForestPlan(points, offsets, queries, query_offsets, k, leaf=leaf,
+                                  boxsize=boxsize, queries_per_block=qb)
+                try:
+                    plan.run()
+                    plan.check()
+                    times = []
+                    for _ in range(reps):
+                        e0 = torch.cuda.Event(enable_timing=True)
+                        e1 = torch.cuda.Event(enable_timing=True)
+                        e0.record()
+                        plan.run()
+                        e1.record()
+                        plan.check()
+                        times.append(e0.elapsed_time(e1))
+                    res = (plan.dist.clone(), plan.idx.clone())
+                finally:
+                    plan.close()
+                if ref is None:
+                    ref = res
+                if not _same(res, ref):
+                    raise RuntimeError(f"autotune: forest plan leaf={leaf} qblock={qb} differs")
+                results.append({"config": {"leaf": leaf, "queries_per_block": qb},
+                                "ms": float(np.median(times))})
+        best = min(results, key=lambda r: r["ms"])
+        cand = {f"{r['config']['leaf']}/{r['config']['queries_per_block']}": r["ms"]
+                for r in results}
+        self.cache[key] = {"config": best["config"], "ms": best["ms"], "tried": len(results),
+                           "candidates_ms": cand, "when": time.strftime("%Y-%m-%d %H:%M:%S")}
+        if save:
+            self.save()
+        out = dict(best["config"])
+        out.update(key=key, ms=best["ms"], candidates_ms=cand, cached=False)
+        return out
+
+
 def _same(a, b) -> bool:
     if a is None or b is None:
         return a is b

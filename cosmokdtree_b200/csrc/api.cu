@@ -43,6 +43,9 @@ static std::atomic<int> g_mlp_tc{1};
 bool mlp_tensor_cores() { return g_mlp_tc.load(std::memory_order_relaxed) != 0; }
 static std::atomic<int> g_box_warp{1};
 bool box_warp_enabled() { return g_box_warp.load(std::memory_order_relaxed) != 0; }
+// persistent forest launch: how long an idle CTA polls the work queue (ms), and
+// how many first items the host withholds (0 outside tests)
+static std::atomic<int> g_pk_wait_ms{20000}, g_pk_withhold{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ------------------------------------------------------------ kernel timing
@@ -550,6 +553,14 @@ ckd_status ckd_set_tuning(int key, int value) {
       if (value < 0) return fail(CKD_ERR_BAD_ARG, "pool cap must be >= 0 MiB");
       g_pool_cap.store((int64_t)value << 20);
       return CKD_OK;
+    case 10:
+      if (value < 1 || value > 600000) return fail(CKD_ERR_BAD_ARG, "queue wait must be 1..600000 ms");
+      g_pk_wait_ms.store(value);
+      return CKD_OK;
+    case 11:
+      if (value < 0) return fail(CKD_ERR_BAD_ARG, "withheld items must be >= 0");
+      g_pk_withhold.store(value);
+      return CKD_OK;
 
   }
   return fail(CKD_ERR_BAD_ARG, "unknown tuning key");
@@ -791,6 +802,65 @@ ckd_status ckd_box_fill_host(const ckd_tree* t, const double* boxes, int64_t nb,
 ckd_status ckd_exclusive_scan(const int64_t* in, int64_t* out, int64_t n, void* stream) {
   if (n < 0 || !out || (n > 0 && !in)) return fail(CKD_ERR_BAD_ARG, "bad scan arguments");
   return scan_i64(in, out, n, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- persistent forest plans
+namespace ckd {
+struct ForestPlan;
+ckd_status forest_plan_create(const double* pts_dev, const int64_t* offsets, int64_t T, int d,
+                              int leaf, const double* boxsize, const double* q_dev,
+                              const int64_t* q_offsets, int64_t nq, int k, int sorted,
+                              double* dist_dev, int64_t* idx_dev, double node_factor,
+                              int qblock, ForestPlan** out);
+ckd_status forest_plan_run(ForestPlan* p, cudaStream_t s, int withhold, long long spin_limit);
+ckd_status forest_plan_status(ForestPlan* p, cudaStream_t s);
+const ckd_tree* forest_plan_tree(const ForestPlan* p);
+void forest_plan_release(ForestPlan* p);
+}  // namespace ckd
+
+extern "C" {
+
+ckd_status ckd_forest_plan_create(const double* pts_dev, const int64_t* offsets_host,
+                                  int64_t n_trees, int d, int leaf, const double* boxsize,
+                                  const double* q_dev, const int64_t* q_offsets_host, int64_t nq,
+                                  int k, int sorted, double* dist_dev, int64_t* idx_dev,
+                                  double node_factor, int queries_per_block,
+                                  ckd_forest_plan** out) {
+  if (!out) return fail(CKD_ERR_BAD_ARG, "null output handle pointer");
+  *out = nullptr;
+  int dev = 0;
+  CKD_TRY(check_device(&dev));
+  ForestPlan* p = nullptr;
+  CKD_TRY(forest_plan_create(pts_dev, offsets_host, n_trees, d, leaf, boxsize, q_dev,
+                             q_offsets_host, nq, k, sorted, dist_dev, idx_dev, node_factor,
+                             queries_per_block, &p));
+  *out = reinterpret_cast<ckd_forest_plan*>(p);
+  return CKD_OK;
+}
+
+ckd_status ckd_forest_plan_run(ckd_forest_plan* plan, void* stream) {
+  if (!plan) return fail(CKD_ERR_BAD_ARG, "null plan");
+  const long long polls = (long long)g_pk_wait_ms.load() * 2000;
+  return forest_plan_run(reinterpret_cast<ForestPlan*>(plan), (cudaStream_t)stream,
+                         g_pk_withhold.load(), polls);
+}
+
+ckd_status ckd_forest_plan_status(ckd_forest_plan* plan, void* stream) {
+  if (!plan) return fail(CKD_ERR_BAD_ARG, "null plan");
+  return forest_plan_status(reinterpret_cast<ForestPlan*>(plan), (cudaStream_t)stream);
+}
+
+ckd_status ckd_forest_plan_forest(const ckd_forest_plan* plan, const ckd_tree** forest) {
+  if (!plan || !forest) return fail(CKD_ERR_BAD_ARG, "null plan or output");
+  *forest = forest_plan_tree(reinterpret_cast<const ForestPlan*>(plan));
+  return CKD_OK;
+}
+
+ckd_status ckd_forest_plan_free(ckd_forest_plan* plan) {
+  forest_plan_release(reinterpret_cast<ForestPlan*>(plan));
+  return CKD_OK;
 }
 
 }  // extern "C"

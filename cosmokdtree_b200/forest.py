@@ -12,6 +12,16 @@ single-tree result, with ids local to the tree.
     forest = build_forest(points, offsets, leaf=16, boxsize=1.0)
     dist, idx = forest.knn(queries, query_offsets, k=8)      # CUDA tensors
     offs, ids = forest.box_csr(boxes, box_offsets)
+
+``ForestPlan`` does the build and the kNN of a whole forest in ONE persistent
+launch driven by a device work queue of (tree, level) and (tree, query block)
+items; ``run()`` allocates nothing and does not synchronise, so it can be captured
+in a CUDA graph and replayed:
+
+    plan = ForestPlan(points, offsets, queries, query_offsets, k=8, boxsize=1.0)
+    plan.run(); plan.check()                    # or capture plan.run() in a graph
+    dist, idx = plan.dist, plan.idx
+    offs, ids = plan.forest().box_csr(boxes, box_offsets)
 """
 from __future__ import annotations
 
@@ -24,7 +34,7 @@ from . import _lib
 from ._lib import CKDArgumentError, check
 from .kdtree import _check_k, _on_device, _ptr, _stream
 
-__all__ = ["Forest", "build_forest"]
+__all__ = ["Forest", "ForestPlan", "build_forest"]
 
 
 def _offsets(off, n_trees=None, total=None, what="offsets") -> np.ndarray:
@@ -214,3 +224,87 @@ def build_forest(points, offsets=None, leaf=16, boxsize=None) -> Forest:
             _ptr(pts), off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(off) - 1, d, dtype,
             leaf, boxp, 1, _stream(), ctypes.byref(h)))
     return Forest(h, off, d, leaf, box, device)
+
+
+class _PlanForest(Forest):
+    """The forest a ForestPlan built (its arrays belong to the plan)."""
+
+    def close(self):
+        self._h = None
+
+
+class ForestPlan:
+    """Build a forest and answer its kNN queries in one persistent launch.
+
+    ``points`` (N, d) and ``queries`` (nq, d) are float64 CUDA tensors (kept by
+    reference and read at every ``run``), rows grouped by tree with host offsets;
+    results land in ``self.dist`` / ``self.idx`` (nq, k), ids local to the tree,
+    exactly the rows ``build_forest(...).knn(...)`` returns."""
+
+    def __init__(self, points, offsets, queries, query_offsets, k, leaf=16, boxsize=None,
+                 sorted=True, node_factor=0.0, queries_per_block=128):
+        k = _check_k(k)
+        if not (_on_device(points) and _on_device(queries)):
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "points and queries must be CUDA tensors")
+        if points.dim() != 2 or queries.dim() != 2 or queries.shape[1] != points.shape[1]:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM, "points and queries must be (n, d)")
+        self.device = points.device.index
+        self.points = points.to(torch.float64).contiguous()
+        self.queries = queries.to(device=points.device, dtype=torch.float64).contiguous()
+        n, d = self.points.shape
+        nq = self.queries.shape[0]
+        self.offsets = _offsets(offsets, total=n)
+        self.query_offsets = _offsets(query_offsets, len(self.offsets) - 1, nq, "query offsets")
+        self.n_trees = len(self.offsets) - 1
+        self.d, self.k, self.leaf = d, k, int(leaf)
+        box = None
+        if boxsize is not None:
+            box = np.full(d, float(boxsize)) if np.ndim(boxsize) == 0 else \
+                np.array(boxsize, dtype=np.float64)
+        self.boxsize = box
+        self.dist = torch.empty((nq, k), dtype=torch.float64, device=points.device)
+        self.idx = torch.empty((nq, k), dtype=torch.int64, device=points.device)
+        self._h = None
+        h = ctypes.c_void_p()
+        P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))  # noqa: E731
+        with torch.cuda.device(self.device):
+            boxp = box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if box is not None else None
+            check(_lib.load().ckd_forest_plan_create(
+                _ptr(self.points), P(self.offsets), self.n_trees, d, self.leaf, boxp,
+                _ptr(self.queries), P(self.query_offsets), nq, k, int(bool(sorted)),
+                _ptr(self.dist), _ptr(self.idx), float(node_factor), int(queries_per_block),
+                ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "plan has been freed")
+        return self._h
+
+    def run(self):
+        """Enqueue the launch on the current stream (no allocation, no sync)."""
+        with torch.cuda.device(self.device):
+            check(_lib.load().ckd_forest_plan_run(self.handle, _stream()))
+
+    def check(self):
+        """Synchronise and raise if the last run failed (CKDTimeout, CKDOutOfMemory...)."""
+        with torch.cuda.device(self.device):
+            check(_lib.load().ckd_forest_plan_status(self.handle, _stream()))
+
+    def forest(self) -> Forest:
+        """The forest of the last successful run, for box and ball searches."""
+        h = ctypes.c_void_p()
+        check(_lib.load().ckd_forest_plan_forest(self.handle, ctypes.byref(h)))
+        return _PlanForest(h, self.offsets, self.d, self.leaf, self.boxsize, self.device)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.load().ckd_forest_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -125,7 +125,12 @@ ckd_status ckd_set_knn_variant(int variant);
  * (1 = a warp per box, frontier expanded a level at a time, default; 0 = a lane
  * per box); key 9: cap in MiB on the device memory the library's pool hands out
  * at any time on the current device (0 = none, default): an allocation past it
- * fails with CKD_ERR_OOM and the call returns everything it had taken. */
+ * fails with CKD_ERR_OOM and the call returns everything it had taken; key 10:
+ * how long (ms, default 20000) an idle CTA of the persistent forest launch waits
+ * for work before it gives up with CKD_ERR_TIMEOUT; key 11: number of first work
+ * items the host withholds from the persistent forest launch while counting them
+ * as pending (default 0; a test of the bounded wait: the launch cannot finish
+ * and ends with CKD_ERR_TIMEOUT). */
 ckd_status ckd_set_tuning(int key, int value);
 
 /* Bytes of the current device's library pool in use by live allocations (trees,
@@ -243,6 +248,40 @@ ckd_status ckd_forest_info(const ckd_tree* forest, int64_t* n_trees, int64_t* of
 ckd_status ckd_forest_knn(const ckd_tree* forest, const double* q_dev, const int64_t* q_offsets_dev,
                           int64_t nq, int k, int sorted, double* dist_dev, int64_t* idx_dev,
                           void* stream);
+/* One persistent launch that builds a whole forest and answers its kNN queries
+ * (no reference counterpart: the reference builds one tree per call and searches
+ * it query by query, src/cosmokdtree.f90:124-238 and :504-540).  Every CTA of a
+ * resident grid takes items from a device work queue: (tree, level) items split
+ * the tree's open nodes of that level (the sliding-midpoint rule of
+ * src/cosmokdtree.f90:347-410, the same trees as ckd_forest_build), and once a
+ * tree is complete its (tree, query block) items search it (exact kNN, k <= 64,
+ * rows in query order).  Idle CTAs poll the queue with a bounded wait
+ * (ckd_set_tuning key 10); running past it ends the launch with CKD_ERR_TIMEOUT.
+ *
+ * ckd_forest_plan_create allocates everything once (cudaMalloc; points and
+ * queries stay the caller's device arrays, read at every run; offsets on the
+ * host; node_factor <= 0 sizes the node arrays for 0.45 nodes per point;
+ * queries_per_block 32..2^20, e.g. 128).  ckd_forest_plan_run enqueues the
+ * launch without allocating or synchronising, so it can be captured in a CUDA
+ * graph (a first uncaptured run sets the kernel attributes).
+ * ckd_forest_plan_status synchronises the stream and returns the launch's
+ * status (CKD_ERR_OOM: node capacity exceeded, recreate with a larger factor;
+ * CKD_ERR_DEPTH: a tree deeper than 126 levels; CKD_ERR_TIMEOUT); after a
+ * successful status, ckd_forest_plan_forest gives the built forest (owned by the
+ * plan, valid until the next run or ckd_forest_plan_free; never pass it to
+ * ckd_free) for the box and ball searches. */
+typedef struct ckd_forest_plan ckd_forest_plan;
+ckd_status ckd_forest_plan_create(const double* pts_dev, const int64_t* offsets_host,
+                                  int64_t n_trees, int d, int leaf, const double* boxsize,
+                                  const double* q_dev, const int64_t* q_offsets_host, int64_t nq,
+                                  int k, int sorted, double* dist_dev, int64_t* idx_dev,
+                                  double node_factor, int queries_per_block,
+                                  ckd_forest_plan** out);
+ckd_status ckd_forest_plan_run(ckd_forest_plan* plan, void* stream);
+ckd_status ckd_forest_plan_status(ckd_forest_plan* plan, void* stream);
+ckd_status ckd_forest_plan_forest(const ckd_forest_plan* plan, const ckd_tree** forest);
+ckd_status ckd_forest_plan_free(ckd_forest_plan* plan);
+
 /* Box search over a forest, boxes grouped by tree like the kNN queries
  * (b_offsets_dev, device, n_trees + 1 entries); two-phase CSR as ckd_box_*. */
 ckd_status ckd_forest_box_count(const ckd_tree* forest, const double* boxes_dev,
