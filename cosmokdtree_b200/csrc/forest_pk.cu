@@ -7,14 +7,16 @@
 // subvolumes) would leave the GPU idle between per-tree launches, so here every
 // CTA of one resident grid takes items from a queue in global memory:
 //
-//   (tree t, level l)  split every open node of tree t at depth l: the
+//   (tree t, level l, group g)  split open nodes of tree t at depth l: the
 //       sliding-midpoint rule of cosmokdtree.f90:347-410 (longest cell side,
 //       ties to the larger spread, midpoint, slide to the extreme point when a
 //       side would be empty) and a stable partition (:455-497 up to the order of
 //       equal keys, which is canonical here: the lowest original index first).
-//       Nodes of 2048 points or more are split by the whole CTA, smaller ones by
-//       a warp each.  If open nodes remain, the CTA pushes (t, l + 1); otherwise
-//       tree t is complete and it pushes t's query blocks.
+//       A level is cut into groups (one open node of 2048+ points, split by the
+//       whole CTA, or up to 128 smaller nodes, a warp each) so that the levels
+//       of large trees spread over many CTAs.  The last group of a level to
+//       finish pushes the next level's groups, or, when no node is left open,
+//       tree t's query blocks.
 //   (tree t, query block b)  the exact kNN of up to `qblock` of t's queries:
 //       one query per lane, the per-lane traversal with the compact heap
 //       (ckd_knn_lane.cuh) started at t's root.
@@ -51,7 +53,9 @@ constexpr int kPkWarps = kPkThreads / 32;
 constexpr int kPkItems = 4;          // positions per thread per pass of a CTA-wide split
 constexpr int kBigNode = 2048;       // nodes this large are split by the whole CTA
 constexpr int kPkMaxDepth = kLaneStack - 2;  // deepest node the per-lane search can hold
-constexpr int kPkMaxLevels = 256;    // queue slots reserved per tree for its levels
+constexpr int kPkMaxLevels = 256;    // deepest level a tree may reach
+constexpr int kPkGroupNodes = 128;   // small open nodes per group item of a level
+constexpr int kPkMaxGroups = 512;    // group items per level of one tree
 constexpr unsigned long long kItemBuild = 1ull, kItemQuery = 2ull;
 
 struct PkState {
@@ -83,7 +87,8 @@ struct PkArgs {
   int32_t* I[2];
   int32_t* lists;       // per tree: two halves of open-node ids (big from the front)
   const int64_t* lbase; // per tree: offset of its halves in `lists`
-  int2* tcnt;           // per tree: (big, small) open nodes of its next level
+  int2* tcnt;           // per tree, per level parity: (big, small) open nodes listed
+  int32_t* tdone;       // per tree: group items of its current level that finished
   float* tslack;        // [tree][d]: screen slack of the tree (max |coordinate| + L)
   const int64_t* off;   // point offsets (T + 1)
   const int64_t* qoff;  // query offsets (T + 1)
@@ -683,17 +688,32 @@ __device__ bool root_init(const PkArgs& a, int t, SideStats<D>* shs, int* s_bad)
   return !lf;
 }
 
-// Push what follows tree t's level l (thread 0): the next level, or the queries.
-__device__ void after_level(const PkArgs& a, int t, int l, int nb, int ns) {
+// Group items of a level with nb big and ns small open nodes: a big node each,
+// or kPkGroupNodes small nodes each, at most kPkMaxGroups.
+__device__ __forceinline__ int level_groups(int nb, int ns) {
+  const int g = max(nb, (ns + kPkGroupNodes - 1) / kPkGroupNodes);
+  return max(1, min(g, kPkMaxGroups));
+}
+
+// Called by thread 0 of each group item of tree t's level l once its work is
+// written and fenced.  The last group to finish pushes what follows: the next
+// level's group items, or, when no node is left open, t's query blocks.
+__device__ void level_done(const PkArgs& a, int t, int l, int groups) {
+  if (atomicAdd(&a.tdone[t], 1) != groups - 1) return;
+  __threadfence();  // the other groups' list entries and counts are visible now
+  a.tdone[t] = 0;
+  int* nx = reinterpret_cast<int*>(a.tcnt + 2 * t + ((l + 1) & 1));
+  const int nb = atomicAdd(nx, 0), ns = atomicAdd(nx + 1, 0);
+  a.tcnt[2 * t + (l & 1)] = make_int2(0, 0);  // free for level l + 2's list
+  __threadfence();
   if (nb + ns > 0) {
     if (l + 1 >= kPkMaxLevels) {
       pk_fail(a, CKD_ERR_DEPTH);
       return;
     }
-    a.tcnt[t] = make_int2(nb, ns);
-    __threadfence();
-    atomicAdd(reinterpret_cast<unsigned long long*>(&a.st->outstanding), 1ull);
-    pk_push(a, kItemBuild, t, (uint32_t)(l + 1), 1);
+    const int g = level_groups(nb, ns);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&a.st->outstanding), (unsigned long long)g);
+    pk_push(a, kItemBuild, t, (uint32_t)(l + 1) << 16, (uint32_t)g);
     return;
   }
   const int64_t nq = __ldcg(a.qoff + t + 1) - __ldcg(a.qoff + t);
@@ -704,9 +724,10 @@ __device__ void after_level(const PkArgs& a, int t, int l, int nb, int ns) {
   pk_push(a, kItemQuery, t, 0, nblk);
 }
 
+// Group g of tree t's level l; returns the level's number of groups.
 template <int D, bool PER>
-__device__ void pk_level(const PkArgs& a, int t, int l, int* s_nb, int* s_ns, BlockShared& bsh,
-                         SideStats<D>* shs, int* s_bad) {
+__device__ int pk_level(const PkArgs& a, int t, int l, int g, BlockShared& bsh,
+                        SideStats<D>* shs, int* s_bad) {
   const int cur = l & 1;
   const double* Xc = a.X[cur];
   const int32_t* Ic = a.I[cur];
@@ -717,38 +738,39 @@ __device__ void pk_level(const PkArgs& a, int t, int l, int* s_nb, int* s_ns, Bl
   const int64_t lb = __ldcg(a.lbase + t);
   const int32_t* list_cur = a.lists + lb + cur * lcap;
   int32_t* list_nxt = a.lists + lb + (cur ^ 1) * lcap;
-  if (threadIdx.x == 0) {
-    *s_nb = 0;
-    *s_ns = 0;
-  }
-  __syncthreads();
-  int nb, ns;
+  // the next level's list counts, shared by every group of this level
+  int* nxt = reinterpret_cast<int*>(a.tcnt + 2 * t + (cur ^ 1));
+  int nb, ns, groups;
   if (l == 0) {
     if (!root_init<D, PER>(a, t, shs, s_bad)) {
       __syncthreads();
-      return;
+      return 1;
     }
     nb = (s1 - s0) >= kBigNode ? 1 : 0;
     ns = 1 - nb;
+    groups = 1;
   } else {
-    const int2 c = __ldcg(a.tcnt + t);
+    const int2 c = __ldcg(a.tcnt + 2 * t + cur);
     nb = c.x;
     ns = c.y;
+    groups = level_groups(nb, ns);
   }
-  for (int i = 0; i < nb; ++i) {
+  for (int i = g; i < nb; i += groups) {
     const int32_t nd = l == 0 ? t : __ldcg(list_cur + i);
-    split_block<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, s_nb, s_ns, bsh, shs);
+    split_block<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, nxt, nxt + 1, bsh, shs);
     if (threadIdx.x == 0) *s_bad = pk_error(a);
     __syncthreads();
-    if (*s_bad) return;  // the whole CTA leaves together
+    if (*s_bad) return groups;  // the whole CTA leaves together
   }
   const int w = threadIdx.x >> 5;
-  for (int i = w; i < ns; i += kPkWarps) {
+  const int i0 = (int)((int64_t)g * ns / groups), i1 = (int)((int64_t)(g + 1) * ns / groups);
+  for (int i = i0 + w; i < i1; i += kPkWarps) {
     const int32_t nd = l == 0 ? t : __ldcg(list_cur + lcap - 1 - i);
-    split_warp<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, s_nb, s_ns);
+    split_warp<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, nxt, nxt + 1);
   }
   __threadfence();
   __syncthreads();
+  return groups;
 }
 
 template <int D, bool PER>
@@ -773,7 +795,7 @@ template <int D, bool PER>
 __global__ void __launch_bounds__(kPkThreads, 4) k_forest_pk(PkArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long s_item;
-  __shared__ int s_nb, s_ns, s_bad;
+  __shared__ int s_bad;
   __shared__ BlockShared bsh;
   __shared__ SideStats<D> shs[kPkWarps];
   TreeView tv = a.tv;
@@ -788,8 +810,9 @@ __global__ void __launch_bounds__(kPkThreads, 4) k_forest_pk(PkArgs a) {
     const int t = (int)((item >> 32) & 0x3fffffffull);
     const uint32_t pl = (uint32_t)(item & 0xffffffffull);
     if (type == kItemBuild) {
-      pk_level<D, PER>(a, t, (int)pl, &s_nb, &s_ns, bsh, shs, &s_bad);
-      if (threadIdx.x == 0 && !pk_error(a)) after_level(a, t, (int)pl, s_nb, s_ns);
+      const int l = (int)(pl >> 16), g = (int)(pl & 0xffffu);
+      const int groups = pk_level<D, PER>(a, t, l, g, bsh, shs, &s_bad);
+      if (threadIdx.x == 0 && !pk_error(a)) level_done(a, t, l, groups);
     } else {
       pk_queries<D, PER>(a, tv, t, pl, heaps);
       __threadfence();
@@ -859,6 +882,7 @@ struct ForestPlan {
   int64_t* lbase = nullptr;
   int32_t* lists = nullptr;
   int2* tcnt = nullptr;
+  int32_t* tdone = nullptr;
   float* tslack = nullptr;
   int32_t* roots = nullptr;
   int32_t* ext = nullptr;
@@ -889,6 +913,8 @@ ckd_status pk_launch(ForestPlan* p, cudaStream_t s, int withhold, long long spin
   const int T = (int)p->T;
   ckd_tree* t = p->tree;
   const unsigned rb = (unsigned)cdiv(std::max<int64_t>(p->queue_cap, 1), 256);
+  CKD_CUDA(cudaMemsetAsync(p->tcnt, 0, sizeof(int2) * 2 * T, s));
+  CKD_CUDA(cudaMemsetAsync(p->tdone, 0, sizeof(int32_t) * T, s));
   k_pk_reset<<<rb, 256, 0, s>>>(p->st, p->queue, p->queue_cap, p->roots, T, withhold);
   CKD_LAUNCH_CHECK();
   k_pk_points<<<(unsigned)cdiv(p->n, 256), 256, 0, s>>>(p->pts_in, p->n, D, p->off, T, p->X[0],
@@ -916,6 +942,7 @@ ckd_status pk_launch(ForestPlan* p, cudaStream_t s, int withhold, long long spin
   a.lists = p->lists;
   a.lbase = p->lbase;
   a.tcnt = p->tcnt;
+  a.tdone = p->tdone;
   a.tslack = p->tslack;
   a.off = p->off;
   a.qoff = p->qoff;
@@ -1023,7 +1050,11 @@ ckd_status forest_plan_create(const double* pts_dev, const int64_t* offsets, int
     p->L[j] = boxsize ? boxsize[j] : 0.0;
   }
   p->node_cap = (int32_t)cap;
-  p->queue_cap = T * (int64_t)kPkMaxLevels + 64;
+  // level items: every tree's levels, a group per kPkGroupNodes small open nodes
+  // (open nodes over all levels are internal nodes, at most half the node
+  // capacity), a group per big open node (at most n / kBigNode per level)
+  p->queue_cap = T * (int64_t)kPkMaxLevels + (int64_t)(cap / 2) / kPkGroupNodes +
+                 32 * (n / kBigNode) + 64;
   for (int64_t i = 0; i < T; ++i) p->queue_cap += (qo[i + 1] - qo[i] + qblock - 1) / qblock;
   p->off_h = off;
   // list halves per tree: at most (points / (leaf + 1) + 2) open nodes per level
@@ -1071,7 +1102,8 @@ ckd_status forest_plan_create(const double* pts_dev, const int64_t* offsets, int
   CKD_CUDA(plan_alloc(p, &p->qoff, sizeof(int64_t) * (T + 1)));
   CKD_CUDA(plan_alloc(p, &p->lbase, sizeof(int64_t) * T));
   CKD_CUDA(plan_alloc(p, &p->lists, sizeof(int32_t) * ltot));
-  CKD_CUDA(plan_alloc(p, &p->tcnt, sizeof(int2) * T));
+  CKD_CUDA(plan_alloc(p, &p->tcnt, sizeof(int2) * 2 * T));
+  CKD_CUDA(plan_alloc(p, &p->tdone, sizeof(int32_t) * T));
   CKD_CUDA(plan_alloc(p, &p->tslack, sizeof(float) * d * T));
   CKD_CUDA(plan_alloc(p, &p->roots, sizeof(int32_t) * T));
   CKD_CUDA(plan_alloc(p, &p->queue, sizeof(unsigned long long) * p->queue_cap));
