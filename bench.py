@@ -47,6 +47,13 @@ WORKLOADS = {
     "clustered_periodic_2p22_k32": (1 << 22, 32, True, 16, 1),
 }
 DEFAULT_WORKLOAD = "clustered_periodic_2p24_k32"
+# DRAM bytes (read + write) of one launch of the default kNN kernel per query, from
+# an ncu capture of the 2^22-point form of the default workload (4.02 GB per
+# 2^22-query launch, profiles/knn_lane2_clustered_2p22_k32.md); the traffic of a
+# launch grows with its queries (each reads its neighbourhood and writes its row)
+KNN_DRAM_BYTES_PER_QUERY = 4.02e9 / (1 << 22)
+KNN_TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2^22-point "
+                    "case, scaled by the query count")
 # learned-bound configurations with their own query sets (several k, other dims)
 MULTI_WORKLOADS = {
     # 2^26 clustered periodic, 10^7 queries (half particles, half uniform), k in {8,32,64}
@@ -987,10 +994,12 @@ def main():
         ab = otree.knn_algbytes(Ph[samp], k, od[:, -1] ** 2)
         bytes_per_q = ab["bytes"] / len(samp)
 
-        def roof(ms, kernel):
+        def roof(ms, kernel, traffic_per_q=None):
             a = bytes_per_q * nq / (ms / 1e3) / 1e9
             return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
-                    "traffic": None, "kernel": kernel, "kernel_ms": ms,
+                    "traffic": None if traffic_per_q is None else traffic_per_q * nq,
+                    "traffic_note": None if traffic_per_q is None else KNN_TRAFFIC_NOTE,
+                    "kernel": kernel, "kernel_ms": ms,
                     "alg_bytes_per_query": bytes_per_q, "peak_kind": peak_kind}
 
         cpu = None
@@ -1005,7 +1014,7 @@ def main():
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(name, world),
-            "roofline": roof(plain_kernel_ms, "k_knn_lane2"),
+            "roofline": roof(plain_kernel_ms, "k_knn_lane2", KNN_DRAM_BYTES_PER_QUERY),
             "cpu_baseline": cpu,
             "e2e": {"value": n_all / (e2e_ms_v / 1e3), "unit": "queries/s",
                     "h2d_bytes_per_step": n_all * 3 * 8, "d2h_bytes_per_step": n_all * k * 16,
