@@ -477,8 +477,9 @@ def run_small_uniform(args):
 
 
 def run_multi(args):
-    """Learned-bound vs plain kNN on a configuration with its own queries: several k
-    (queries split evenly, one search call per k), optional 6-D float32 input.  The
+    """Learned-bound vs plain kNN on a configuration with its own queries: a k per
+    query drawn from the configuration's set, every step one mixed-k call (the
+    queries are grouped by k on the device), optional 6-D float32 input.  The
     network is trained on 10^6 exact k-th distances of a separate catalogue of the
     same size and kind (train_seed) with queries drawn the same way."""
     import torch
@@ -531,33 +532,28 @@ def run_multi(args):
     train_s = time.perf_counter() - t0
     ttr.close()
     del Ptr, Qtr
-    # evaluation queries, split evenly over the k values
+    # evaluation queries with a k per query drawn from ks; one mixed-k call per step
     Qh = queries(P, cfg["query_seed"], nq)
-    kq = np.random.default_rng(cfg["query_seed"] + 1).integers(0, len(ks), nq)
-    groups = []
-    for gi, k in enumerate(ks):
-        qg = torch.from_numpy(np.ascontiguousarray(Qh[kq == gi])).cuda()
-        m = qg.shape[0]
-        outs = [(torch.empty((m, k), dtype=torch.float64, device="cuda"),
-                 torch.empty((m, k), dtype=torch.int64, device="cuda")) for _ in range(2)]
-        groups.append((k, qg, outs))
+    kq = np.asarray(ks, dtype=np.int32)[np.random.default_rng(cfg["query_seed"] + 1)
+                                        .integers(0, len(ks), nq)]
+    kmax = int(max(ks))
+    Qd = torch.from_numpy(np.ascontiguousarray(Qh)).cuda()
+    Kd = torch.from_numpy(kq).cuda()
+    outs = [(torch.empty((nq, kmax), dtype=torch.float64, device="cuda"),
+             torch.empty((nq, kmax), dtype=torch.int64, device="cuda")) for _ in range(2)]
     nfb = ctypes.c_int64()
     fallbacks = {}
+    vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
 
     def plain_step():
-        for k, qg, outs in groups:
-            _lib.check(L.ckd_knn(tree.handle, ctypes.c_void_p(qg.data_ptr()), qg.shape[0], k, 1,
-                                 ctypes.c_void_p(outs[0][0].data_ptr()),
-                                 ctypes.c_void_p(outs[0][1].data_ptr()), sp))
+        _lib.check(L.ckd_knn_multi_k(tree.handle, vp(Qd), nq, vp(Kd), kmax, 1, vp(outs[0][0]),
+                                     vp(outs[0][1]), sp))
 
     def learned_step():
-        for k, qg, outs in groups:
-            _lib.check(L.ckd_knn_learned(tree.handle, lb.handle, ctypes.c_void_p(qg.data_ptr()),
-                                         qg.shape[0], k, 1,
-                                         ctypes.c_void_p(outs[1][0].data_ptr()),
-                                         ctypes.c_void_p(outs[1][1].data_ptr()),
-                                         ctypes.byref(nfb), sp))
-            fallbacks[k] = int(nfb.value)
+        _lib.check(L.ckd_knn_learned_multi_k(tree.handle, lb.handle, vp(Qd), nq, vp(Kd), kmax, 1,
+                                             vp(outs[1][0]), vp(outs[1][1]), ctypes.byref(nfb),
+                                             sp))
+        fallbacks["all"] = int(nfb.value)
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -576,8 +572,7 @@ def run_multi(args):
         plain_ms = timed(plain_step)
         learned_ms = timed(learned_step)
     launches = (L.ckd_launch_count() - l0) // (2 * (args.steps + args.warmup))
-    exact = all(torch.equal(o[0][0], o[1][0]) and torch.equal(o[0][1], o[1][1])
-                for _, _, o in groups)
+    exact = bool(torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1]))
     # oracle parity on a sample and CPU baseline
     import oracle
     threads = os.cpu_count() or 1
@@ -586,14 +581,16 @@ def run_multi(args):
     cpu_build_s = time.perf_counter() - t0
     parity = True
     cpu_q, cpu_s = 0, 0.0
-    for k, qg, outs in groups:
-        qs = qg[:2000].cpu().numpy()
+    for k in ks:
+        rows = np.nonzero(kq == k)[0][:2000]
+        qs = Qh[rows]
         t1 = time.perf_counter()
         od, oi = ot.knn(qs, k)
         cpu_s += time.perf_counter() - t1
         cpu_q += len(qs)
-        parity = parity and np.array_equal(oi, outs[1][1][:2000].cpu().numpy()) and \
-            np.array_equal(od, outs[1][0][:2000].cpu().numpy())
+        rsel = torch.from_numpy(rows).cuda()
+        parity = parity and np.array_equal(oi, outs[1][1][rsel, :k].cpu().numpy()) and \
+            np.array_equal(od, outs[1][0][rsel, :k].cpu().numpy())
     ot.close()
     out = {
         "metric": "knn_queries_per_s", "value": nq / (learned_ms / 1e3), "unit": "queries/s",
@@ -607,8 +604,9 @@ def run_multi(args):
         "plain": {"value": nq / (plain_ms / 1e3), "ms_per_step": plain_ms},
         "learned": {"value": nq / (learned_ms / 1e3), "speedup_vs_plain": plain_ms / learned_ms,
                     "exact_vs_plain": bool(exact),
-                    "fallback_rate": {str(k): fallbacks[k] / max(1, g[1].shape[0])
-                                      for k, g in zip(ks, groups)},
+                    "fallback_rate": fallbacks["all"] / nq,
+                    "calls_per_step": "one mixed-k call (ckd_knn_multi_k / "
+                                      "ckd_knn_learned_multi_k)",
                     "train_s": train_s, "margin_log2": fit["margin"],
                     "holdout_rms_log2": fit["holdout_rms_log2"]},
         "cpu_baseline": {"value": cpu_q / cpu_s, "unit": "queries/s", "cores": threads,

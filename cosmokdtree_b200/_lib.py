@@ -124,6 +124,7 @@ SIGNATURES = {
     "ckd_mlp_train": [_vp, _vp, _vp, _i64, _int, _int, ctypes.c_float, _vp, _vp],
     "ckd_mlp_predict": [_vp, _vp, _i64, _vp, _vp],
     "ckd_knn_learned": [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp, _vp],
+    "ckd_knn_learned_multi_k": [_vp, _vp, _vp, _i64, _vp, _int, _int, _vp, _vp, _vp, _vp],
 }
 
 MLP_FEATURES = 12

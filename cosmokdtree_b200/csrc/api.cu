@@ -125,7 +125,8 @@ ckd_status build_dispatch(ckd_tree* t, const void* pts_dev, int dtype, cudaStrea
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s);
 ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* kq,
-                       int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s);
+                       int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s,
+                       const ckd_mlp* net = nullptr, int64_t* nfb_out = nullptr);
 ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
                        int sorted, double* dist, int64_t* idx, cudaStream_t s);
 ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
@@ -475,6 +476,22 @@ ckd_status ckd_knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const
   if (!q || !k_dev || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query, k or output pointer");
   if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
   return knn_multi_k(t, q, nq, k_dev, kmax, sorted, dist, idx, (cudaStream_t)stream);
+}
+
+ckd_status ckd_knn_learned_multi_k(const ckd_tree* t, const ckd_mlp* net, const double* q,
+                                   int64_t nq, const int32_t* k_dev, int kmax, int sorted,
+                                   double* dist, int64_t* idx, int64_t* n_fallback,
+                                   void* stream) {
+  CKD_TRY(check_single(t));
+  CKD_TRY(mlp_check(net));
+  if (kmax < 1 || kmax > 65536) return fail(CKD_ERR_BAD_ARG, "kmax must be 1..65536");
+  if (nq < 0) return fail(CKD_ERR_BAD_ARG, "negative query count");
+  if (n_fallback) *n_fallback = 0;
+  if (nq == 0) return CKD_OK;
+  if (!q || !k_dev || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query, k or output pointer");
+  if (nq > INT32_MAX) return fail(CKD_ERR_BAD_ARG, "at most 2^31 - 1 queries per call");
+  return knn_multi_k(t, q, nq, k_dev, kmax, sorted, dist, idx, (cudaStream_t)stream, net,
+                     n_fallback);
 }
 
 ckd_status ckd_query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,

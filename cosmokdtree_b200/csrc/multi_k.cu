@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "ckd_common.cuh"
+#include "ckd_mlp.cuh"
 
 namespace ckd {
 
@@ -95,8 +96,15 @@ ckd_status gather_q(int d, const double* q, const int32_t* rows, int64_t n, doub
 
 }  // namespace
 
+ckd_status knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* q, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, int64_t* nfb, cudaStream_t s);
+
+// net != nullptr: every k group takes the learned-bound search (its reruns are
+// added to *nfb_out).
 ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* kq,
-                       int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+                       int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s,
+                       const ckd_mlp* net, int64_t* nfb_out) {
+  if (nfb_out) *nfb_out = 0;
   int32_t *hist = nullptr, *off = nullptr, *fill = nullptr, *grp = nullptr, *bad = nullptr;
   // every buffer joins the guard as soon as it exists, so a failed allocation
   // returns the earlier ones to the pool
@@ -148,7 +156,13 @@ ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int
     CKD_CUDA(dev_alloc((void**)&ig, sizeof(int64_t) * n * k, s));
     fr.ps.push_back(ig);
     CKD_TRY(gather_q(t->d, q, rows, n, qg, s));
-    CKD_TRY(knn_run(t, qg, n, k, sorted, dg, ig, s));
+    if (net) {
+      int64_t nfb = 0;
+      CKD_TRY(knn_learned(t, net, qg, n, k, sorted, dg, ig, &nfb, s));
+      if (nfb_out) *nfb_out += nfb;
+    } else {
+      CKD_TRY(knn_run(t, qg, n, k, sorted, dg, ig, s));
+    }
     k_scatter_rows<<<(unsigned)cdiv(n * kmax, 256), 256, 0, s>>>(dg, ig, rows, n, k, kmax, dist,
                                                                 idx);
     CKD_LAUNCH_CHECK();

@@ -228,6 +228,37 @@ class LearnedBound:
         with torch.cuda.device(tree.device):
             return _to_host(dist), _to_host(idx)
 
+    def knn_multi_k(self, tree: KDTree, target, ks, sorted=True):
+        """Exact kNN with a k per target row and the learned bound, in one call:
+        (dist, idx) of shape (ntar, max(ks)) like ``kdtree.knn_search_multi_k``
+        (slots past a row's own k hold id -2); the reruns are counted in
+        ``last_fallback``.  numpy for host input, CUDA tensors for CUDA input."""
+        if tree.device != self.device:
+            raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "tree and network are on different devices")
+        with torch.cuda.device(tree.device):
+            q, _ = _queries(tree, target)
+            nq = q.shape[0]
+            kt = torch.as_tensor(np.asarray(ks) if not isinstance(ks, torch.Tensor) else ks)
+            if kt.dim() != 1 or kt.shape[0] != nq:
+                raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "ks must hold one k per target row")
+            if kt.dtype.is_floating_point or kt.dtype == torch.bool:
+                raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be an integer")
+            kt = kt.to(device=q.device, dtype=torch.int32).contiguous()
+            kmax = int(kt.max().item()) if nq > 0 else 1
+            if nq > 0 and int(kt.min().item()) < 1:
+                raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG, "k must be a positive integer")
+            dist = torch.empty((nq, kmax), dtype=torch.float64, device=q.device)
+            idx = torch.empty((nq, kmax), dtype=torch.int64, device=q.device)
+            nfb = ctypes.c_int64()
+            if nq > 0:
+                check(_lib.load().ckd_knn_learned_multi_k(
+                    tree.handle, self.handle, _ptr(q), nq, _ptr(kt), kmax, int(bool(sorted)),
+                    _ptr(dist), _ptr(idx), ctypes.byref(nfb), _stream()))
+            self.last_fallback = int(nfb.value)
+            if isinstance(target, torch.Tensor) and target.is_cuda:
+                return dist, idx
+            return _to_host(dist), _to_host(idx)
+
     def knn_batch(self, tree: KDTree, target, k, sorted=True):
         """As ``knn`` with CUDA-tensor results."""
         k = _check_k(k)

@@ -366,6 +366,16 @@ ckd_status ckd_knn_learned(const ckd_tree* tree, const ckd_mlp* net, const doubl
                            int64_t nq, int k, int sorted, double* dist_dev, int64_t* idx_dev,
                            int64_t* n_fallback, void* stream);
 
+/* ckd_knn_multi_k with the learned bound: the queries are grouped by k on the
+ * device as there, and each group takes the ckd_knn_learned search (no
+ * reference counterpart).  Rows equal ckd_knn_multi_k's; *n_fallback is the
+ * total number of queries that reran without the bound.  Reads the k histogram
+ * and each group's rerun count back (synchronises). */
+ckd_status ckd_knn_learned_multi_k(const ckd_tree* tree, const ckd_mlp* net, const double* q_dev,
+                                   int64_t nq, const int32_t* k_dev, int kmax, int sorted,
+                                   double* dist_dev, int64_t* idx_dev, int64_t* n_fallback,
+                                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -159,6 +159,11 @@ def test_gpu_config_c4_mixed_k_and_learned(gpu, oracle):
     ttr = kd.build_kdtree(torch.from_numpy(Ptr).cuda(), leaf=16, boxsize=1.0)
     lb = LearnedBound(seed=0)
     lb.fit(ttr, synth.mixed_queries(Ptr, 60_000, seed=5), [8, 32, 64], epochs=4, batch=4096)
+    # the whole mixed batch in one learned-bound call equals the plain mixed-k call
+    md, mi = lb.knn_multi_k(t, Q, ks)
+    np.testing.assert_array_equal(mi, i)
+    np.testing.assert_array_equal(md, d)
+    assert 0 <= lb.last_fallback < nq
     for kk in (8, 32, 64):
         rows = np.nonzero(ks == kk)[0]
         ld, li = lb.knn(t, Q[rows], kk)
