@@ -300,6 +300,16 @@ __device__ __forceinline__ void knn_lane_run(
     }
   }
   if (stats) {
+    // slots 4 and 7: 32 x the warp's largest leaf-scan and node-test counts, so that
+    // against slots 2 and 0 (every lane's) they show how long lanes wait for the
+    // slowest query of their warp
+    unsigned long long m2 = st[2], m0 = st[0];
+    for (int o = 16; o > 0; o >>= 1) {
+      m2 = max(m2, __shfl_xor_sync(FULL, m2, o));
+      m0 = max(m0, __shfl_xor_sync(FULL, m0, o));
+    }
+    st[4] = lane == 0 ? 32 * m2 : 0;
+    st[7] = lane == 0 ? 32 * m0 : 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       unsigned long long v = st[c];
