@@ -334,13 +334,27 @@ __device__ __forceinline__ void decide(const double* bx, const double* cl, const
   }
 }
 
+// What one group item gathers in shared memory and publishes once at its end: the
+// leaves it made and its open children for the next level's list (the hot global
+// counters are touched once per item, not once per split; entries past the
+// buffers go straight to the global list).
+constexpr int kAccBig = 64;
+constexpr int kAccSmall = 2 * kPkGroupNodes + 16;
+struct ItemAcc {
+  int nleaves;
+  int nbig;
+  int nsmall;
+  int32_t big[kAccBig];
+  int32_t small[kAccSmall];
+};
+
 // Records of a split node and its two children, then the children's place in
 // the next level (called by one thread).
 template <int D>
 __device__ void finish_split(const PkArgs& a, int t, int32_t nd, const NodeMeta& m,
                              const double* cl, int axis, double mid, int32_t cid, int32_t nl,
                              const SideStats<D>& sl, const SideStats<D>& sr, int32_t* list_nxt,
-                             int64_t lcap, int* s_nb, int* s_ns) {
+                             int64_t lcap, int* s_nb, int* s_ns, ItemAcc& acc) {
   constexpr int NV = (D + 3) / 4;
   constexpr int PF = pair_f4(D);
   const int32_t cnt[2] = {nl, m.count - nl};
@@ -356,11 +370,19 @@ __device__ void finish_split(const PkArgs& a, int t, int32_t nd, const NodeMeta&
     const bool lf = cnt[side] <= a.leaf;
     write_node<D>(a, cid + side, st0[side], cnt[side], m.depth + 1, nd, side ? sr : sl, cc, lf);
     if (lf) {
-      atomicAdd(&a.st->n_leaves, 1);
+      atomicAdd(&acc.nleaves, 1);
     } else if (cnt[side] >= kBigNode) {
-      list_nxt[atomicAdd(s_nb, 1)] = cid + side;
+      const int i = atomicAdd(&acc.nbig, 1);
+      if (i < kAccBig)
+        acc.big[i] = cid + side;
+      else
+        list_nxt[atomicAdd(s_nb, 1)] = cid + side;
     } else {
-      list_nxt[lcap - 1 - atomicAdd(s_ns, 1)] = cid + side;
+      const int i = atomicAdd(&acc.nsmall, 1);
+      if (i < kAccSmall)
+        acc.small[i] = cid + side;
+      else
+        list_nxt[lcap - 1 - atomicAdd(s_ns, 1)] = cid + side;
     }
   }
   NodeMeta mm = m;
@@ -387,8 +409,6 @@ __device__ void finish_split(const PkArgs& a, int t, int32_t nd, const NodeMeta&
   rec[4 * NV] = *reinterpret_cast<const float4*>(&info);
   const int4 range = make_int4(st0[0], cnt[0], st0[1], cnt[1]);
   rec[4 * NV + 1] = *reinterpret_cast<const float4*>(&range);
-  atomicMax(&a.st->max_depth, m.depth + 1);
-  if (m.depth + 1 > kPkMaxDepth) pk_fail(a, CKD_ERR_DEPTH);
   (void)t;
 }
 
@@ -413,9 +433,9 @@ __device__ __forceinline__ void load_node(const PkArgs& a, int32_t nd, int d2, N
 // ---------------------------------------------------------------- splits
 // One node split by one warp.
 template <int D>
-__device__ void split_warp(const PkArgs& a, int t, int32_t nd, const double* Xc, const int32_t* Ic,
-                           double* Xn, int32_t* In, int32_t* list_nxt, int64_t lcap, int* s_nb,
-                           int* s_ns) {
+__device__ void split_warp(const PkArgs& a, int t, int32_t nd, int32_t cid, const double* Xc,
+                           const int32_t* Ic, double* Xn, int32_t* In, int32_t* list_nxt,
+                           int64_t lcap, int* s_nb, int* s_ns, ItemAcc& acc) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t n = a.tv.n;
@@ -440,13 +460,6 @@ __device__ void split_warp(const PkArgs& a, int t, int32_t nd, const double* Xc,
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     nl = c;
   }
-  int32_t cid = 0;
-  if (lane == 0) {
-    cid = atomicAdd(&a.st->nodes, 2);
-    if (cid + 2 > a.node_cap) pk_fail(a, CKD_ERR_OOM);
-  }
-  cid = __shfl_sync(0xffffffffu, cid, 0);
-  if (cid + 2 > a.node_cap) return;
   const bool leafL = nl <= a.leaf, leafR = m.count - nl <= a.leaf;
   SideStats<D> sl, sr;
   stats_init(sl);
@@ -486,7 +499,7 @@ __device__ void split_warp(const PkArgs& a, int t, int32_t nd, const double* Xc,
   stats_warp_reduce(sl);
   stats_warp_reduce(sr);
   if (lane == 0)
-    finish_split<D>(a, t, nd, m, cl, axis, mid, cid, nl, sl, sr, list_nxt, lcap, s_nb, s_ns);
+    finish_split<D>(a, t, nd, m, cl, axis, mid, cid, nl, sl, sr, list_nxt, lcap, s_nb, s_ns, acc);
 }
 
 // Exclusive prefix over the CTA of per-(pass, warp) counts, in position order
@@ -520,9 +533,10 @@ struct BlockShared {
 
 // One node split by the whole CTA.
 template <int D>
-__device__ void split_block(const PkArgs& a, int t, int32_t nd, const double* Xc, const int32_t* Ic,
-                            double* Xn, int32_t* In, int32_t* list_nxt, int64_t lcap, int* s_nb,
-                            int* s_ns, BlockShared& sh, SideStats<D>* shs) {
+__device__ void split_block(const PkArgs& a, int t, int32_t nd, int32_t cid, const double* Xc,
+                            const int32_t* Ic, double* Xn, int32_t* In, int32_t* list_nxt,
+                            int64_t lcap, int* s_nb, int* s_ns, BlockShared& sh,
+                            SideStats<D>* shs, ItemAcc& acc) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t n = a.tv.n;
@@ -552,14 +566,6 @@ __device__ void split_block(const PkArgs& a, int t, int32_t nd, const double* Xc
     __syncthreads();
     nl = sh.cnt;
   }
-  if (threadIdx.x == 0) {
-    int32_t cid = atomicAdd(&a.st->nodes, 2);
-    if (cid + 2 > a.node_cap) pk_fail(a, CKD_ERR_OOM);
-    sh.cid = cid;
-  }
-  __syncthreads();
-  const int32_t cid = sh.cid;
-  if (cid + 2 > a.node_cap) return;  // uniform
   const bool leafL = nl <= a.leaf, leafR = m.count - nl <= a.leaf;
   SideStats<D> sl, sr;
   stats_init(sl);
@@ -618,7 +624,7 @@ __device__ void split_block(const PkArgs& a, int t, int32_t nd, const double* Xc
   stats_block_reduce(sl, shs);
   stats_block_reduce(sr, shs);
   if (threadIdx.x == 0)
-    finish_split<D>(a, t, nd, m, cl, axis, mid, cid, nl, sl, sr, list_nxt, lcap, s_nb, s_ns);
+    finish_split<D>(a, t, nd, m, cl, axis, mid, cid, nl, sl, sr, list_nxt, lcap, s_nb, s_ns, acc);
   __syncthreads();
 }
 
@@ -724,10 +730,13 @@ __device__ void level_done(const PkArgs& a, int t, int l, int groups) {
   pk_push(a, kItemQuery, t, 0, nblk);
 }
 
-// Group g of tree t's level l; returns the level's number of groups.
+// Group g of tree t's level l; returns the level's number of groups.  Every open
+// node is split exactly once, so the group takes the child ids of all its nodes
+// with one atomic; leaves, depth and the open children are published once at the
+// end.
 template <int D, bool PER>
 __device__ int pk_level(const PkArgs& a, int t, int l, int g, BlockShared& bsh,
-                        SideStats<D>* shs, int* s_bad) {
+                        SideStats<D>* shs, int* s_bad, ItemAcc& acc, int* s_base) {
   const int cur = l & 1;
   const double* Xc = a.X[cur];
   const int32_t* Ic = a.I[cur];
@@ -755,19 +764,47 @@ __device__ int pk_level(const PkArgs& a, int t, int l, int g, BlockShared& bsh,
     ns = c.y;
     groups = level_groups(nb, ns);
   }
-  for (int i = g; i < nb; i += groups) {
+  const int mybig = nb > g ? (nb - g + groups - 1) / groups : 0;  // i = g, g + groups, ...
+  const int i0 = (int)((int64_t)g * ns / groups), i1 = (int)((int64_t)(g + 1) * ns / groups);
+  const int mine = mybig + (i1 - i0);
+  if (threadIdx.x == 0) {
+    acc.nleaves = acc.nbig = acc.nsmall = 0;
+    const int base = mine > 0 ? atomicAdd(&a.st->nodes, 2 * mine) : 0;
+    if (mine > 0 && (int64_t)base + 2 * mine > a.node_cap) pk_fail(a, CKD_ERR_OOM);
+    if (mine > 0 && l + 1 > kPkMaxDepth) pk_fail(a, CKD_ERR_DEPTH);
+    *s_base = base;
+    *s_bad = pk_error(a);
+  }
+  __syncthreads();
+  if (*s_bad) return groups;  // the whole CTA leaves together
+  const int32_t base = *s_base;
+  for (int i = g, j = 0; i < nb; i += groups, ++j) {
     const int32_t nd = l == 0 ? t : __ldcg(list_cur + i);
-    split_block<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, nxt, nxt + 1, bsh, shs);
-    if (threadIdx.x == 0) *s_bad = pk_error(a);
-    __syncthreads();
-    if (*s_bad) return groups;  // the whole CTA leaves together
+    split_block<D>(a, t, nd, base + 2 * j, Xc, Ic, Xn, In, list_nxt, lcap, nxt, nxt + 1, bsh,
+                   shs, acc);
   }
   const int w = threadIdx.x >> 5;
-  const int i0 = (int)((int64_t)g * ns / groups), i1 = (int)((int64_t)(g + 1) * ns / groups);
   for (int i = i0 + w; i < i1; i += kPkWarps) {
     const int32_t nd = l == 0 ? t : __ldcg(list_cur + lcap - 1 - i);
-    split_warp<D>(a, t, nd, Xc, Ic, Xn, In, list_nxt, lcap, nxt, nxt + 1);
+    split_warp<D>(a, t, nd, base + 2 * (mybig + i - i0), Xc, Ic, Xn, In, list_nxt, lcap, nxt,
+                  nxt + 1, acc);
   }
+  __syncthreads();
+  // publish: the group's open children into the next level's list, its leaves
+  // and depth into the launch's counts
+  if (threadIdx.x == 0) {
+    const int kb = min(acc.nbig, kAccBig), ks = min(acc.nsmall, kAccSmall);
+    acc.nbig = kb ? atomicAdd(nxt, kb) : 0;         // now: first list slot of each kind
+    acc.nsmall = ks ? atomicAdd(nxt + 1, ks) : 0;
+    bsh.tl = kb;
+    bsh.tr = ks;
+    if (acc.nleaves) atomicAdd(&a.st->n_leaves, acc.nleaves);
+    if (mine > 0) atomicMax(&a.st->max_depth, l + 1);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < bsh.tl; i += kPkThreads) list_nxt[acc.nbig + i] = acc.big[i];
+  for (int i = threadIdx.x; i < bsh.tr; i += kPkThreads)
+    list_nxt[lcap - 1 - (acc.nsmall + i)] = acc.small[i];
   __threadfence();
   __syncthreads();
   return groups;
@@ -795,7 +832,8 @@ template <int D, bool PER>
 __global__ void __launch_bounds__(kPkThreads, 4) k_forest_pk(PkArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long s_item;
-  __shared__ int s_bad;
+  __shared__ int s_bad, s_base;
+  __shared__ ItemAcc acc;
   __shared__ BlockShared bsh;
   __shared__ SideStats<D> shs[kPkWarps];
   TreeView tv = a.tv;
@@ -811,7 +849,7 @@ __global__ void __launch_bounds__(kPkThreads, 4) k_forest_pk(PkArgs a) {
     const uint32_t pl = (uint32_t)(item & 0xffffffffull);
     if (type == kItemBuild) {
       const int l = (int)(pl >> 16), g = (int)(pl & 0xffffu);
-      const int groups = pk_level<D, PER>(a, t, l, g, bsh, shs, &s_bad);
+      const int groups = pk_level<D, PER>(a, t, l, g, bsh, shs, &s_bad, acc, &s_base);
       if (threadIdx.x == 0 && !pk_error(a)) level_done(a, t, l, groups);
     } else {
       pk_queries<D, PER>(a, tv, t, pl, heaps);
