@@ -4,8 +4,9 @@ Every kNN kernel variant returns the same exact result, so the choice is purely
 about speed and depends on the data (dimension, clustering, periodicity), k and
 the GPU.  ``Autotuner.tune`` times a grid of configurations on a sample of the
 user's own points and queries -- leaf size (tree build), kernel variant (which
-also fixes where the k-heaps live: per-lane shared-memory heaps, packet
-traversal heaps, warp-per-bucket lists, or the caller's output rows for k > 64),
+also fixes how a node is expanded: per-lane compact heaps descending by
+bounding boxes or by child-pair records; the packet traversal and the caller's
+output rows for k > 64 are the fallbacks the automatic choice keeps),
 warps per block, a cap on resident blocks per SM, and whether queries are
 ordered by leaf -- checks that every candidate returns the baseline's result
 bit for bit, and caches the fastest per (d, k, dtype, periodic, size class, GPU)
@@ -36,7 +37,7 @@ _KEY_VARIANT, _KEY_BPS, _KEY_WPB, _KEY_ORDER = 0, 1, 2, 6
 
 DEFAULT_GRID = {
     "leaf": (8, 16, 32),
-    "variant": (9, 7, 8),
+    "variant": (7, 8),
     "warps_per_block": (1, 2, 4),
     "blocks_per_sm": (0,),
     "order": (0,),

@@ -518,8 +518,8 @@ int64_t ckd_launch_count(void) { return g_launches.load(); }
 ckd_status ckd_knn_stats(int enable, int64_t* out8) { return knn_stats(enable, out8); }
 
 ckd_status ckd_set_knn_variant(int variant) {
-  if (!(variant == 0 || variant == 1 || variant == 7 || variant == 8 || variant == 9))
-    return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0, 1, 7, 8 or 9");
+  if (!(variant == 0 || variant == 1 || variant == 7 || variant == 8))
+    return fail(CKD_ERR_BAD_ARG, "kNN variant must be 0, 1, 7 or 8");
   g_knn_variant.store(variant);
   return CKD_OK;
 }
@@ -550,8 +550,8 @@ ckd_status ckd_set_tuning(int key, int value) {
       g_knn_wpb.store(value);
       return CKD_OK;
     case 4:
-      if (!(value == 0 || value == 3 || value == 4))
-        return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0, 3 or 4");
+      if (!(value == 0 || value == 3))
+        return fail(CKD_ERR_BAD_ARG, "learned kernel must be 0 or 3");
       g_learned_kernel.store(value);
       return CKD_OK;
     case 6:

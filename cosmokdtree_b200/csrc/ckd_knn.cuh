@@ -259,14 +259,4 @@ __device__ __forceinline__ void compact_write(const TreeView& tv, const uint2* H
 
 CKD_LD_END
 
-// The warp-converged kNN kernel (knn_warp.cu).  Returns false without launching
-// when the tree or k is outside its limits (the caller then uses another kernel).
-bool knn_warp_supported(const ckd_tree* t, int k);
-template <int D, bool PER>
-ckd_status knn_warp_launch(const ckd_tree* t, const double* q, const int32_t* order,
-                           const int32_t* qleaf, const int32_t* qroot, int64_t nq, int k,
-                           int sorted, double* dist, int64_t* idx, const double* r2,
-                           int32_t* miss, unsigned* nmiss, unsigned long long* stats,
-                           cudaStream_t s);
-
 }  // namespace ckd

@@ -308,14 +308,14 @@ __global__ void k_bucket_scatter(const int32_t* __restrict__ key, int64_t nq,
 }
 
 // Kernel choice (ckd_set_knn_variant): 0 automatic, 1 FP64 packet traversal,
-// 7 per-lane compact heap, 8 the same expanding nodes from child-pair records,
-// 9 warp-converged (needs the queries in leaf order).  Automatic takes 8;
+// 7 per-lane compact heap, 8 the same expanding nodes from child-pair records.
+// Automatic takes 8;
 // trees too deep for its stack, coordinates beyond the FP32 screen's range and
 // k > 64 take the packet kernel.
 template <int D, bool PER>
-ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
-                      const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
-                      int64_t* idx, cudaStream_t s, int force_variant = -1) {
+ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
+                      int sorted, double* dist, int64_t* idx, cudaStream_t s,
+                      int force_variant = -1) {
   TreeView tv = t->view();
   const int var = force_variant >= 0 ? force_variant : knn_variant();
   if (force_variant < 0) timing_begin(s);
@@ -326,9 +326,6 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
       if (on) timing_end(s);
     }
   } timing_guard{s, force_variant < 0};
-  if (var == 9 && order && qleaf && knn_warp_supported(t, k))
-    return knn_warp_launch<D, PER>(t, q, order, qleaf, nullptr, nq, k, sorted, dist, idx, nullptr,
-                                   nullptr, nullptr, knn_stats_buffer(), s);
   if (k <= kSmemK && t->screen_ok && var != 1 && t->depth < kLaneStack - 1) {
     const int nw7 = std::min(4, knn_warps_per_block());
     const unsigned blocks7 = (unsigned)cdiv(cdiv(nq, 32), nw7);
@@ -381,11 +378,10 @@ ckd_status knn_launch(const ckd_tree* t, const double* q, const int32_t* order,
 }
 
 template <int D>
-ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* order,
-                          const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
-                          int64_t* idx, cudaStream_t s) {
-  if (t->periodic) return knn_launch<D, true>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-  return knn_launch<D, false>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+ckd_status knn_dispatch_d(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq,
+                          int k, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
+  if (t->periodic) return knn_launch<D, true>(t, q, order, nq, k, sorted, dist, idx, s);
+  return knn_launch<D, false>(t, q, order, nq, k, sorted, dist, idx, s);
 }
 
 template <int D>
@@ -413,8 +409,6 @@ ckd_status order_impl(const ckd_tree* t, const double* q, int64_t nq, int32_t* o
   return CKD_OK;
 }
 
-// Warp-per-bucket search: locate + counting sort, bucket list, bucket kernel,
-// then the per-lane kernel for any query the bucket rounds left unresolved.
 }  // namespace
 
 ckd_status knn_stats(int enable, int64_t* out) {
@@ -431,23 +425,14 @@ ckd_status knn_stats(int enable, int64_t* out) {
 }
 
 ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                       int32_t* qleaf, cudaStream_t s) {
+                       cudaStream_t s) {
   switch (t->d) {
-    case 1: return order_impl<1>(t, q, nq, order, qleaf, s);
-    case 2: return order_impl<2>(t, q, nq, order, qleaf, s);
-    case 3: return order_impl<3>(t, q, nq, order, qleaf, s);
-    case 4: return order_impl<4>(t, q, nq, order, qleaf, s);
-    case 5: return order_impl<5>(t, q, nq, order, qleaf, s);
-    case 6: return order_impl<6>(t, q, nq, order, qleaf, s);
-    case 7: return order_impl<7>(t, q, nq, order, qleaf, s);
-    case 8: return order_impl<8>(t, q, nq, order, qleaf, s);
+#define CKD_QO(DD) \
+  case DD: return order_impl<DD>(t, q, nq, order, nullptr, s);
+    CKD_QO(1) CKD_QO(2) CKD_QO(3) CKD_QO(4) CKD_QO(5) CKD_QO(6) CKD_QO(7) CKD_QO(8)
+#undef CKD_QO
   }
   return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
-}
-
-ckd_status query_order(const ckd_tree* t, const double* q, int64_t nq, int32_t* order,
-                       cudaStream_t s) {
-  return query_order(t, q, nq, order, nullptr, s);
 }
 
 // leaf order of queries that each start at their own tree's root (forests)
@@ -471,45 +456,30 @@ bool want_order(const ckd_tree* t, int64_t nq) {
   return nq >= 4096 && nq * 8 >= t->n / 64;
 }
 
-ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order,
-                       const int32_t* qleaf, int64_t nq, int k, int sorted, double* dist,
-                       int64_t* idx, cudaStream_t s) {
+ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
+                       int sorted, double* dist, int64_t* idx, cudaStream_t s) {
   switch (t->d) {
-    case 1: return knn_dispatch_d<1>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 2: return knn_dispatch_d<2>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 3: return knn_dispatch_d<3>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 4: return knn_dispatch_d<4>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 5: return knn_dispatch_d<5>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 6: return knn_dispatch_d<6>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 7: return knn_dispatch_d<7>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
-    case 8: return knn_dispatch_d<8>(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+    case 1: return knn_dispatch_d<1>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 2: return knn_dispatch_d<2>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 3: return knn_dispatch_d<3>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 4: return knn_dispatch_d<4>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 5: return knn_dispatch_d<5>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 6: return knn_dispatch_d<6>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 7: return knn_dispatch_d<7>(t, q, order, nq, k, sorted, dist, idx, s);
+    case 8: return knn_dispatch_d<8>(t, q, order, nq, k, sorted, dist, idx, s);
   }
   return fail(CKD_ERR_BAD_DIM, "dimensionality must be 1..8");
 }
 
-ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
-                       int sorted, double* dist, int64_t* idx, cudaStream_t s) {
-  return knn_ordered(t, q, order, nullptr, nq, k, sorted, dist, idx, s);
-}
-
 ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted, double* dist,
                    int64_t* idx, cudaStream_t s) {
+  Scratch sc(s);
   int32_t* order = nullptr;
-  int32_t* qleaf = nullptr;
-  struct Free {
-    int32_t** p[2];
-    cudaStream_t s;
-    ~Free() {
-      for (int32_t** x : p)
-        if (*x) dev_free(*x, s);
-    }
-  } free_guard{{&order, &qleaf}, s};
   if (want_order(t, nq)) {
-    CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
-    CKD_CUDA(dev_alloc((void**)&qleaf, sizeof(int32_t) * nq, s));
-    CKD_TRY(query_order(t, q, nq, order, qleaf, s));
+    CKD_CUDA(sc.alloc(&order, sizeof(int32_t) * nq));
+    CKD_TRY(query_order(t, q, nq, order, s));
   }
-  return knn_ordered(t, q, order, qleaf, nq, k, sorted, dist, idx, s);
+  return knn_ordered(t, q, order, nq, k, sorted, dist, idx, s);
 }
 
 // ===================================================================
@@ -521,37 +491,22 @@ namespace {
 template <int D, bool PER>
 ckd_status forest_knn_impl(const ckd_tree* t, const double* q, const int32_t* qroot, int64_t nq,
                            int k, int sorted, double* dist, int64_t* idx, cudaStream_t s) {
-  int32_t *order = nullptr, *qleaf = nullptr;
-  struct Free {
-    int32_t** p[2];
-    cudaStream_t s;
-    ~Free() {
-      for (int32_t** x : p)
-        if (*x) dev_free(*x, s);
-    }
-  } free_guard{{&order, &qleaf}, s};
-  CKD_CUDA(dev_alloc((void**)&order, sizeof(int32_t) * nq, s));
-  CKD_CUDA(dev_alloc((void**)&qleaf, sizeof(int32_t) * nq, s));
-  CKD_TRY(order_impl<D>(t, q, nq, order, qleaf, s, nullptr, qroot));
+  Scratch sc(s);
+  int32_t* order = nullptr;
+  CKD_CUDA(sc.alloc(&order, sizeof(int32_t) * nq));
+  CKD_TRY(order_impl<D>(t, q, nq, order, nullptr, s, nullptr, qroot));
   timing_begin(s);
-  if (knn_variant() == 9 && knn_warp_supported(t, k)) {
-    const ckd_status st = knn_warp_launch<D, PER>(t, q, order, qleaf, qroot, nq, k, sorted, dist,
-                                                  idx, nullptr, nullptr, nullptr,
-                                                  knn_stats_buffer(), s);
-    if (st != CKD_OK) return st;
-  } else {
-    const int nw = std::min(4, knn_warps_per_block());
-    const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
-    size_t sm = (size_t)nw * compact_heap_bytes(k);
-    const int bps = knn_blocks_per_sm();
-    if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
-    CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sm));
-    k_knn_lane2<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist, idx,
-                                                    knn_stats_buffer(), nullptr, nullptr, nullptr,
-                                                    nullptr, qroot);
-    CKD_LAUNCH_CHECK();
-  }
+  const int nw = std::min(4, knn_warps_per_block());
+  const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
+  size_t sm = (size_t)nw * compact_heap_bytes(k);
+  const int bps = knn_blocks_per_sm();
+  if (bps > 0) sm = std::max(sm, (size_t)(200 * 1024) / bps);
+  CKD_CUDA(cudaFuncSetAttribute(k_knn_lane2<D, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+  k_knn_lane2<D, PER><<<blocks, nw * 32, sm, s>>>(t->view(), q, order, nq, k, sorted, dist, idx,
+                                                  knn_stats_buffer(), nullptr, nullptr, nullptr,
+                                                  nullptr, qroot);
+  CKD_LAUNCH_CHECK();
   timing_end(s);
   return CKD_OK;
 }
@@ -603,10 +558,7 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     timing_begin(s);
     st = mlp_radius(t, net, q, order, qleaf, nq, k, r2, s);
   }
-  if (st == CKD_OK && learned_kernel() == 4 && knn_warp_supported(t, k)) {
-    st = knn_warp_launch<D, PER>(t, q, order, qleaf, nullptr, nq, k, sorted, dist, idx, r2, miss,
-                                 nmiss, knn_stats_buffer(), s);
-  } else if (st == CKD_OK) {
+  if (st == CKD_OK) {
     const int nw = std::min(4, knn_warps_per_block());
     const unsigned blocks = (unsigned)cdiv(cdiv(nq, 32), nw);
     size_t sm = (size_t)nw * compact_heap_bytes(k);
@@ -637,7 +589,7 @@ ckd_status knn_learned_impl(const ckd_tree* t, const ckd_mlp* net, const double*
     else if ((int64_t)nm > nq) st = fail(CKD_ERR_CUDA, "internal error: fallback list overflow");
   }
   if (st == CKD_OK && nm > 0)
-    st = knn_launch<D, PER>(t, q, miss, nullptr, (int64_t)nm, k, sorted, dist, idx, s, 7);
+    st = knn_launch<D, PER>(t, q, miss, (int64_t)nm, k, sorted, dist, idx, s, 7);
   if (st == CKD_OK) timing_end(s);
   if (nfb_out) *nfb_out = nm;
   return st;

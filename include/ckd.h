@@ -106,10 +106,8 @@ int64_t ckd_launch_count(void);
  * when k <= 64, the coordinates allow the FP32 screen and the tree is shallow
  * enough; 1 otherwise), 1 = FP64 packet
  * traversal, 7 = per-lane traversal with 8-byte heap entries (FP32 key +
- * position, exact tie resolution), 8 = 7 expanding nodes from child-pair records,
- * 9 = warp-converged search (a warp walks the tree once for 32 queries adjacent
- * in leaf order and screens each visited leaf for all of them).  Every variant
- * returns the same exact result. */
+ * position, exact tie resolution), 8 = 7 expanding nodes from child-pair records.
+ * Every variant returns the same exact result. */
 ckd_status ckd_set_knn_variant(int variant);
 
 /* Process-wide launch tuning of the search kernels (no reference counterpart;
@@ -117,8 +115,7 @@ ckd_status ckd_set_knn_variant(int variant);
  * key 1: cap on resident blocks per SM for the per-lane kNN kernel (0 = as many
  * as fit); key 2: warps per block of the per-lane kNN kernel (1..8, default 2,
  * at most 4 used); key 4: search kernel of ckd_knn_learned (0 = bounded per-lane
- * traversal; 3 = 0 with child-pair-record descent, default; 4 = bounded
- * warp-converged search); key 6: ordering of queries by leaf before kNN and ball
+ * traversal; 3 = 0 with child-pair-record descent, default); key 6: ordering of queries by leaf before kNN and ball
  * searches (0 = automatic, default; 1 = always; 2 = never); key 7: inference of
  * the learned-bound network (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on
  * BF16 activations, default); key 8: box search of up to 32768 boxes per call

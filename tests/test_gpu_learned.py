@@ -88,8 +88,8 @@ def test_features_match_numpy(gpu):
     np.testing.assert_allclose(f, ref, rtol=0, atol=2e-4)
 
 
-@pytest.fixture(params=[0, 3, 4],
-                ids=["bounded_lane_compact", "bounded_lane_pair", "bounded_warp"])
+@pytest.fixture(params=[0, 3],
+                ids=["bounded_lane_compact", "bounded_lane_pair"])
 def learned_kernel(request, gpu):
     from cosmokdtree_b200 import _lib
     _lib.check(_lib.load().ckd_set_tuning(4, request.param))
@@ -178,19 +178,15 @@ def test_learned_bound_saves_work(trained):
     assert learned[6] < 0.8 * plain[6], (learned, plain)
     assert learned[0] < 0.9 * plain[0], (learned, plain)
     assert learned[5] < plain[5], (learned, plain)
-    # warp-converged kernels: fewer inserts and FP64 evaluations
-    _lib.check(L.ckd_set_knn_variant(9))
-    _lib.check(L.ckd_set_tuning(6, 1))
-    _lib.check(L.ckd_set_tuning(4, 4))
+    # child-pair-record kernels (the defaults): fewer inserts and FP64 evaluations
+    _lib.check(L.ckd_set_knn_variant(8))
     try:
-        wplain = stats(lambda: kdtree.knn_search(t, Q, 32))
-        wlearned = stats(lambda: lb.knn(t, Q, 32))
+        pplain = stats(lambda: kdtree.knn_search(t, Q, 32))
+        plearned = stats(lambda: lb.knn(t, Q, 32))
     finally:
         _lib.check(L.ckd_set_knn_variant(0))
-        _lib.check(L.ckd_set_tuning(6, 0))
-        _lib.check(L.ckd_set_tuning(4, 3))
-    assert wlearned[6] < wplain[6], (wlearned, wplain)
-    assert wlearned[5] < wplain[5], (wlearned, wplain)
+    assert plearned[6] < pplain[6], (plearned, pplain)
+    assert plearned[5] < pplain[5], (plearned, pplain)
 
 
 def test_tensor_core_inference_matches_reference(gpu):

@@ -118,19 +118,15 @@ KNN_CASES = [
 ]
 
 
-@pytest.fixture(params=[1, 7, 8, 9, 0],
-                ids=["fp64", "lane_compact", "lane_compact_pair", "warp", "auto"])
+@pytest.fixture(params=[1, 7, 8, 0],
+                ids=["fp64", "lane_compact", "lane_compact_pair", "auto"])
 def knn_variant(request, gpu):
-    """Every kNN kernel of the product.  The warp-converged kernel (9) needs the
-    queries in leaf order, so its case forces the ordering pass (tuning key 6)."""
+    """Every kNN kernel of the product (tuning key 0)."""
     from cosmokdtree_b200 import _lib
     L = _lib.load()
     _lib.check(L.ckd_set_knn_variant(request.param))
-    if request.param == 9:
-        _lib.check(L.ckd_set_tuning(6, 1))
     yield request.param
     L.ckd_set_knn_variant(0)
-    L.ckd_set_tuning(6, 0)
 
 
 @pytest.mark.parametrize("name,n,d,periodic,leaf,nq,k", KNN_CASES)
