@@ -101,7 +101,10 @@ __device__ __forceinline__ void init_query_screen(const TreeView& tv, const doub
 // FP64 distances of the results are recomputed once for the output.  Slot s
 // (1-based) of lane l lives at H[s * 32 + l], so every lane always addresses its
 // own bank pair.  Sentinels: position -1 = (HUGE, id -1), position -2 = (r2,
-// INT32_MAX) for the bounded search.
+// INT32_MAX) for the bounded search.  The first k entries that enter are placed
+// by sifting up from the next free slot (a heap of the entries so far, the
+// sentinels parked in the slots past it), so none of them is sifted down through
+// k sentinels; once k have entered, every new one replaces the root.
 __host__ __device__ inline size_t compact_heap_bytes(int k) { return (size_t)(k + 1) * 32 * 8; }
 
 constexpr int32_t kPosMissing = -1;
@@ -136,6 +139,7 @@ struct CompactHeap {
   unsigned wk;
   int32_t wp;
   float wd32;
+  int cnt;  // entries offered so far while fewer than k (then k)
 };
 
 template <int D, bool PER>
@@ -145,23 +149,60 @@ __device__ __forceinline__ void compact_init(CompactHeap& h, int k, float skey, 
   h.wk = __float_as_uint(skey);
   h.wp = spos;
   h.wd32 = wd32;
+  h.cnt = 0;
 }
 
 // Offer leaf-ordered point p at exact squared distance d2: it enters iff it ranks
 // strictly before the root under (d2, id) (the strict test of cosmokdtree.f90:658
-// in canonical form); the root is replaced and sifted down.  Returns true when
-// the heap changed.
-template <int D, bool PER>
+// in canonical form); while fewer than k have entered it is sifted up from the
+// next free slot, afterwards the root is replaced and sifted down.  Returns true
+// when the heap changed.  BND: a bounded search (its root sentinel is the bound,
+// tested before filling; a HUGE root sentinel is beaten by every point).
+template <int D, bool PER, bool BND = false>
 __device__ __forceinline__ bool compact_offer(CompactHeap& h, int k, const CompactCtx<D, PER>& cx,
                                               const double (&q)[D], double d2, int32_t p) {
   const unsigned kc = __float_as_uint(__double2float_rn(d2));
-  if (kc > h.wk) return false;
-  if (kc == h.wk) {  // FP32 tie with the root: exact comparison
-    const double dr = cx.exact(q, h.wp);
-    if (d2 > dr) return false;
-    if (d2 == dr && CKD_LDT(&cx.tv.ids[p]) >= cx.id(h.wp)) return false;
-  }
+  // the entry test against the root: for a bounded search the root is the bound's
+  // sentinel from the start; otherwise it is a HUGE sentinel, which every point
+  // beats, until the heap is full
+  auto beats_root = [&]() -> bool {
+    if (kc > h.wk) return false;
+    if (kc == h.wk) {  // FP32 tie with the root: exact comparison
+      const double dr = cx.exact(q, h.wp);
+      if (d2 > dr) return false;
+      if (d2 == dr && CKD_LDT(&cx.tv.ids[p]) >= cx.id(h.wp)) return false;
+    }
+    return true;
+  };
+  if (BND && !beats_root()) return false;
   uint2* H = h.H;
+  if (h.cnt < k) {
+    // filling: the root is still a sentinel (HUGE, or the bound of a bounded
+    // search); sift up from slot cnt + 1 over the real entries, slots past cnt
+    // keep their sentinels until the heap is full
+    int s = ++h.cnt;
+    while (s > 1) {
+      const int par = s >> 1;
+      const uint2 pe = H[par * 32];
+      bool up = kc > pe.x;  // the candidate ranks after its parent
+      if (kc == pe.x) {
+        const double dp = cx.exact(q, (int32_t)pe.y);
+        up = d2 > dp || (d2 == dp && CKD_LDT(&cx.tv.ids[p]) > cx.id((int32_t)pe.y));
+      }
+      if (!up) break;
+      H[s * 32] = pe;
+      s = par;
+    }
+    H[s * 32] = make_uint2(kc, (unsigned)p);
+    if (h.cnt == k) {
+      const uint2 root = H[32];
+      h.wk = root.x;
+      h.wp = (int32_t)root.y;
+      h.wd32 = __uint_as_float(h.wk + 1u);
+    }
+    return true;
+  }
+  if (!BND && !beats_root()) return false;
   int s = 1;
   for (;;) {
     const int l = 2 * s;
@@ -193,6 +234,27 @@ __device__ __forceinline__ bool compact_offer(CompactHeap& h, int k, const Compa
   h.wp = (int32_t)root.y;
   h.wd32 = __uint_as_float(h.wk + 1u);
   return true;
+}
+
+// After a search that offered fewer than k points, slots cnt + 1 .. k still hold
+// sentinels below real entries: sift each one up so the k slots form a heap.
+template <int D, bool PER>
+__device__ __forceinline__ void compact_finish(CompactHeap& h, int k, const CompactCtx<D, PER>& cx,
+                                               const double (&q)[D]) {
+  uint2* H = h.H;
+  for (int s0 = h.cnt + 1; s0 <= k; ++s0) {
+    const uint2 e = H[s0 * 32];
+    int s = s0;
+    while (s > 1) {
+      const int par = s >> 1;
+      const uint2 pe = H[par * 32];
+      if (!(e.x > pe.x || (e.x == pe.x && cx.tie_before(q, (int32_t)pe.y, (int32_t)e.y)))) break;
+      H[s * 32] = pe;
+      s = par;
+    }
+    H[s * 32] = e;
+  }
+  h.cnt = k;
 }
 
 // Heap sort into ascending (d2, id) (replaces the quicksort of

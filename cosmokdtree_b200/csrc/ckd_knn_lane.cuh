@@ -124,8 +124,7 @@ __device__ __forceinline__ void knn_lane_run(
     return box_lb(lo, hi);
   };
 
-  int32_t sn[kLaneStack];
-  float sd[kLaneStack];
+  uint2 sk[kLaneStack];  // (node, bound bits): one 8-byte entry per pending subtree
   int top = 0;
   int32_t node = valid ? (qroot ? qroot[qi] : root0) : -1;
   if (BOUNDED && valid && qleaf && spos == kPosBound) {
@@ -165,8 +164,7 @@ __device__ __forceinline__ void knn_lane_run(
         const bool nl = ml <= hp.wd32, nr = mr <= hp.wd32;
         if (nl && nr) {
           const bool lf = ml <= mr;
-          sn[top] = lf ? m.left + 1 : m.left;
-          sd[top] = lf ? mr : ml;
+          sk[top] = make_uint2((unsigned)(lf ? m.left + 1 : m.left), __float_as_uint(lf ? mr : ml));
           ++top;
           node = lf ? m.left : m.left + 1;
         } else if (nl || nr) {
@@ -175,8 +173,9 @@ __device__ __forceinline__ void knn_lane_run(
           node = -1;
           while (top > 0) {
             --top;
-            if (sd[top] <= hp.wd32) {
-              node = sn[top];
+            const uint2 e = sk[top];
+            if (__uint_as_float(e.y) <= hp.wd32) {
+              node = (int32_t)e.x;
               break;
             }
           }
@@ -206,8 +205,7 @@ __device__ __forceinline__ void knn_lane_run(
         int32_t nxt = -1;
         if (nl && nr) {
           const bool lf = ml <= mr;
-          sn[top] = lf ? er : el;
-          sd[top] = lf ? mr : ml;
+          sk[top] = make_uint2((unsigned)(lf ? er : el), __float_as_uint(lf ? mr : ml));
           ++top;
           nxt = lf ? el : er;
         } else if (nl || nr) {
@@ -215,8 +213,9 @@ __device__ __forceinline__ void knn_lane_run(
         } else {
           while (top > 0) {
             --top;
-            if (sd[top] <= hp.wd32) {
-              nxt = sn[top];
+            const uint2 e = sk[top];
+            if (__uint_as_float(e.y) <= hp.wd32) {
+              nxt = (int32_t)e.x;
               break;
             }
           }
@@ -273,12 +272,28 @@ __device__ __forceinline__ void knn_lane_run(
           if (s2 <= thr) mask |= 1u << i;
         }
         if (stats) st[5] += __popc(mask);
-        while (mask) {
-          const int i = __ffs(mask) - 1;
-          mask &= mask - 1;
-          const int32_t p = p0 + i;
-          const double d2 = point_d2_rec<D, PER>(tv, q, p);
-          if (compact_offer<D, PER>(hp, k, cx, q, d2, p) && stats) st[6] += 1;
+        if (BOUNDED) {
+          // two candidates at a time, their FP64 records loaded together (faster
+          // for the bounded search, slower for the plain one)
+          while (mask) {
+            const int i0 = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int i1 = mask ? __ffs(mask) - 1 : i0;
+            mask &= mask - 1;
+            const int32_t pa = p0 + i0, pb = p0 + i1;
+            const double da = point_d2_rec<D, PER>(tv, q, pa);
+            const double db = point_d2_rec<D, PER>(tv, q, pb);
+            if (compact_offer<D, PER, true>(hp, k, cx, q, da, pa) && stats) st[6] += 1;
+            if (i1 != i0 && compact_offer<D, PER, true>(hp, k, cx, q, db, pb) && stats) st[6] += 1;
+          }
+        } else {
+          while (mask) {
+            const int i = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int32_t p = p0 + i;
+            const double d2 = point_d2_rec<D, PER>(tv, q, p);
+            if (compact_offer<D, PER, false>(hp, k, cx, q, d2, p) && stats) st[6] += 1;
+          }
         }
       }
     }
@@ -286,8 +301,9 @@ __device__ __forceinline__ void knn_lane_run(
     int32_t nxt = -1;
     while (top > 0) {
       --top;
-      if (sd[top] <= hp.wd32) {
-        nxt = sn[top];
+      const uint2 e = sk[top];
+      if (__uint_as_float(e.y) <= hp.wd32) {
+        nxt = (int32_t)e.x;
         break;
       }
     }
@@ -328,6 +344,7 @@ __device__ __forceinline__ void knn_lane_run(
       if (missed) miss[base + __popc(missmask & ((1u << lane) - 1u))] = (int32_t)qi;
     }
   }
+  if (hp.cnt < k) compact_finish<D, PER>(hp, k, cx, q);
   if (sorted && valid && !missed) compact_sort<D, PER>(hp.H, k, cx, q);
   __syncwarp();
   compact_write<D, PER>(tv, hp.H - lane, lane, gw, nq, order, q, k, missmask, dist, idx);
