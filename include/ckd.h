@@ -138,11 +138,11 @@ ckd_status ckd_pool_usage(int64_t* used, int64_t* reserved);
 /* Traversal statistics of the kNN kernels (diagnostics, no reference
  * counterpart).  Copies the counters accumulated since the previous call into
  * out8 (if not NULL), clears them, and turns collection on (enable=1) or off.
- * Warp-converged kernel: [0] node expansions, [1] stack pops, [2] leaf scans,
- * [3] points screened (per warp), [4] own leaves scanned first, [5] screen passes
- * (FP64 evaluations, per query), [6] heap inserts (per query), [7] climb steps.
- * Per-lane kernel: [0] node expansions, [2] leaf visits, [3] points screened,
- * [5] screen passes, [6] heap inserts (all per query).  Synchronises the device. */
+ * Per-lane kernels: [0] node expansions, [2] leaf visits, [3] points screened,
+ * [5] screen passes (FP64 evaluations), [6] heap inserts (all summed over queries);
+ * [4] and [7]: 32 x the largest leaf-visit and node-expansion counts of each
+ * warp's lanes, summed over warps (against [2] and [0] they show how long lanes
+ * wait for the slowest query of their warp).  Synchronises the device. */
 ckd_status ckd_knn_stats(int enable, int64_t* out8);
 
 /* Kernel timing (diagnostics, no reference counterpart).  With enable=1 the kNN
