@@ -226,37 +226,71 @@ def knn_search_batch(tree: KDTree, target, k, sorted=True):
 
 
 _PIPE_MIN_ROWS = 1 << 20  # host queries from which the search and the copy-back overlap
-_PIPE_CHUNKS = 8
+_PIPE_CHUNKS = 16
 
 
-def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool, search=None):
-    """Host queries, host results: the queries go to the device at once, then the
-    search runs in row chunks on the current stream while a second stream copies
-    each finished chunk's results into the pinned host arrays (two device buffers in
-    flight), so the result transfer overlaps the search.  ``search(q, n, dist, idx,
-    stream)`` runs one chunk (default: ckd_knn)."""
+def _host_rows(tree: KDTree, target) -> np.ndarray:
+    """Host target points as a C-contiguous (nq, d) FP64 array (a 1-D target is one
+    point, kdtree.py:45-46); the dimensionality is checked against the tree."""
+    q = np.ascontiguousarray(np.atleast_1d(np.asarray(target, dtype=np.float64)))
+    if q.ndim == 1:
+        q = q.reshape(1, -1)
+    if q.ndim != 2 or q.shape[1] != tree.d:
+        raise CKDArgumentError(_lib.CKD_ERR_BAD_DIM,
+                               "target dimensionality does not match the tree")
+    return q
+
+
+def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool, search=None,
+                        chunks: int = _PIPE_CHUNKS):
+    """Host queries, host results, in row chunks: each chunk's queries are copied
+    into one of two pinned staging buffers by the host while the device works on
+    the previous chunks, uploaded and searched on the current stream, and its
+    results copied into the pinned host arrays by a second stream (two device
+    result buffers in flight), so both transfers overlap the search.  The periodic
+    range check runs on the device per chunk into one flag, read once at the end
+    (an out-of-range query raises then, and no result is returned).  ``search(q,
+    n, dist, idx, stream)`` runs one chunk (default: ckd_knn); a search with fixed
+    costs per call takes fewer ``chunks``."""
     L = _lib.load()
     if search is None:
         def search(qc, n, db, ib, st):
             check(L.ckd_knn(tree.handle, _ptr(qc), n, k, int(bool(sorted)), _ptr(db), _ptr(ib),
                             st))
-    q, _ = _queries(tree, target)
-    nq = q.shape[0]
-    rows = -(-nq // _PIPE_CHUNKS)
+    qh = _host_rows(tree, target)
+    nq, d = qh.shape
+    dev = torch.device(f"cuda:{tree.device}")
+    rows = -(-nq // max(1, int(chunks)))
+    q = torch.empty((nq, d), dtype=torch.float64, device=dev)
+    stage = [torch.empty((rows, d), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    uploaded = [None, None]
+    bad = None
+    if tree.periodic:
+        half = torch.as_tensor(tree.boxsize / 2.0, dtype=torch.float64, device=dev)
+        bad = torch.zeros((), dtype=torch.bool, device=dev)
     dist_h = torch.empty((nq, k), dtype=torch.float64, pin_memory=True)
     idx_h = torch.empty((nq, k), dtype=torch.int64, pin_memory=True)
     comp = torch.cuda.current_stream()
     copy = torch.cuda.Stream()
-    bufs = [(torch.empty((rows, k), dtype=torch.float64, device=q.device),
-             torch.empty((rows, k), dtype=torch.int64, device=q.device)) for _ in range(2)]
+    bufs = [(torch.empty((rows, k), dtype=torch.float64, device=dev),
+             torch.empty((rows, k), dtype=torch.int64, device=dev)) for _ in range(2)]
     done = [None, None]
     for c, r0 in enumerate(range(0, nq, rows)):
         r1 = min(nq, r0 + rows)
         b = c % 2
+        if uploaded[b] is not None:
+            uploaded[b].synchronize()  # the staging buffer's previous upload has finished
+        stage[b][: r1 - r0].copy_(torch.from_numpy(qh[r0:r1]))
+        qc = q[r0:r1]
+        qc.copy_(stage[b][: r1 - r0], non_blocking=True)
+        uploaded[b] = torch.cuda.Event()
+        uploaded[b].record(comp)
+        if bad is not None:
+            bad |= ((qc < -half) | (qc > half) | torch.isnan(qc)).any()
         if done[b] is not None:
             comp.wait_event(done[b])  # the buffer's previous copy has finished
         db, ib = bufs[b]
-        search(q[r0:r1], r1 - r0, db, ib, ctypes.c_void_p(comp.cuda_stream))
+        search(qc, r1 - r0, db, ib, ctypes.c_void_p(comp.cuda_stream))
         ready = torch.cuda.Event()
         ready.record(comp)
         copy.wait_event(ready)
@@ -267,6 +301,9 @@ def _knn_host_pipelined(tree: KDTree, target, k: int, sorted: bool, search=None)
         done[b].record(copy)
     copy.synchronize()
     comp.wait_stream(copy)
+    if bad is not None and bool(bad):
+        raise CKDArgumentError(_lib.CKD_ERR_OUT_OF_BOX,
+                               "periodic tree: query points must lie in [-L/2, L/2]")
     return dist_h.numpy(), idx_h.numpy()
 
 

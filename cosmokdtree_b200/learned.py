@@ -25,7 +25,8 @@ import torch
 
 from . import _lib
 from ._lib import MLP_FEATURES, MLP_NORM, MLP_PARAMS, CKDArgumentError, check
-from .kdtree import KDTree, _check_k, _ptr, _queries, _stream, _to_host, knn_search_batch
+from .kdtree import (_PIPE_MIN_ROWS, KDTree, _check_k, _knn_host_pipelined, _ptr, _queries,
+                     _stream, _to_host, knn_search_batch)
 
 __all__ = ["LearnedBound"]
 
@@ -222,6 +223,29 @@ class LearnedBound:
         """Exact kNN with the learned bound: (dist, idx) like ``knn_search``
         (numpy for host input, CUDA tensors for CUDA input).  The number of
         queries that needed the unbounded rerun is left in ``last_fallback``."""
+        if not (isinstance(target, torch.Tensor) and target.is_cuda):
+            k = _check_k(k)
+            nq = np.shape(target)[0] if np.ndim(target) == 2 else 1
+            if nq >= _PIPE_MIN_ROWS:
+                if tree.device != self.device:
+                    raise CKDArgumentError(_lib.CKD_ERR_BAD_ARG,
+                                           "tree and network are on different devices")
+                L = _lib.load()
+                nfb_total = [0]
+
+                def search(qc, n, db, ib, st):  # one chunk of the pipeline
+                    nfb = ctypes.c_int64()
+                    check(L.ckd_knn_learned(tree.handle, self.handle, _ptr(qc), n, k,
+                                            int(bool(sorted)), _ptr(db), _ptr(ib),
+                                            ctypes.byref(nfb), st))
+                    nfb_total[0] += int(nfb.value)
+
+                # 4 chunks: each learned call pays an ordering pass, a radius pass
+                # and a readback of its rerun count
+                with torch.cuda.device(tree.device):
+                    out = _knn_host_pipelined(tree, target, k, sorted, search=search, chunks=4)
+                self.last_fallback = nfb_total[0]
+                return out
         dist, idx = self.knn_batch(tree, target, k, sorted)
         if isinstance(target, torch.Tensor) and target.is_cuda:
             return dist, idx
