@@ -632,6 +632,16 @@ def workload_config(name, world=1):
             "l2": "inputs larger than L2 (tree ~0.6 GB, outputs 8.6 GB per step)"}
 
 
+# DRAM bytes per working point and level of the build's three large kernels (k_seg_box,
+# k_flags, k_scatter), from one ncu capture of each at a mid-depth level of the 16.7M-point
+# clustered build (322.5 + 143.1 + 673.0 MB over ~11.3M working points)
+BUILD_DRAM_BYTES_PER_POINT_LEVEL = 100.8
+BUILD_TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_seg_box, k_flags "
+                      "and k_scatter at one mid-depth level, per working point, scaled by the "
+                      "tree's point-levels (the per-level box, flag and scatter passes each "
+                      "read the working set)")
+
+
 def build_roofline(tree, n, d, ms):
     """Build roofline from the algorithmic bytes of a level-synchronous build: the
     input read once (N·D·8), every point read and written once per level above its
@@ -649,8 +659,10 @@ def build_roofline(tree, n, d, ms):
     alg = n * d * 8 + point_levels * 2 * rec + n * rec
     peak, kind = measured_peaks()
     a = alg / (ms / 1e3) / 1e9
+    traffic = BUILD_DRAM_BYTES_PER_POINT_LEVEL * point_levels if d == 3 else None
     return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
-            "traffic": None, "alg_bytes": alg, "point_levels_per_point": point_levels / n,
+            "traffic": traffic, "traffic_note": BUILD_TRAFFIC_NOTE if traffic else None,
+            "alg_bytes": alg, "point_levels_per_point": point_levels / n,
             "kernel": "whole build (all levels)", "peak_kind": kind}
 
 
