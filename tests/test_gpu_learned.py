@@ -220,3 +220,21 @@ def test_tensor_core_inference_matches_reference(gpu):
             np.testing.assert_array_equal(d1, d0)
     finally:
         _lib.check(L.ckd_set_tuning(7, 1))
+
+
+def test_learned_host_pipeline_is_exact(trained):
+    """Host queries from 2^20 rows on take the chunked pipeline (each chunk a learned
+    call with its own reruns); rows equal the plain search's and the rerun count is
+    summed over the chunks."""
+    from cosmokdtree_b200 import kdtree
+    t, P, lb, _ = trained
+    rng = np.random.default_rng(77)
+    nq = kdtree._PIPE_MIN_ROWS + 321
+    Q = np.concatenate([P[rng.integers(0, len(P), nq // 2)],
+                        rng.random((nq - nq // 2, 3)) - 0.5])
+    ld, li = lb.knn(t, Q, 32)
+    assert isinstance(li, np.ndarray) and li.shape == (nq, 32)
+    assert 0 <= lb.last_fallback < 0.2 * nq
+    pd, pi = kdtree.knn_search(t, Q, 32)
+    np.testing.assert_array_equal(li, pi)
+    np.testing.assert_array_equal(ld, pd)
