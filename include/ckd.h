@@ -180,7 +180,10 @@ ckd_status ckd_knn_multi_k(const ckd_tree* tree, const double* q_dev, int64_t nq
                            const int32_t* k_dev, int kmax, int sorted, double* dist_dev,
                            int64_t* idx_dev, void* stream);
 
-/* ckd_knn on host buffers (copies in, computes, copies out; synchronous). */
+/* ckd_knn on host buffers (copies in, computes, copies out; synchronous).  From
+ * 2^20 queries on, the search runs in 16 row chunks while a second stream copies
+ * each finished chunk back (fastest with pinned output buffers; pageable ones
+ * still overlap each copy with the next chunk's search). */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);
 

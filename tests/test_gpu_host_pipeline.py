@@ -43,3 +43,35 @@ def test_gpu_host_pipeline_rejects_out_of_box_queries(gpu):
     d, i = kd.knn_search(t, Q[:1000], 4)
     assert (i >= 0).all()
     t.close()
+
+
+def test_gpu_c_abi_host_pipeline(gpu):
+    """ckd_knn_host from 2^20 queries on runs chunked with the copy-back overlapped:
+    pageable (numpy) and pinned output buffers both give the device path's rows."""
+    import ctypes
+
+    import torch
+    from cosmokdtree_b200 import _lib
+    kd = gpu.kdtree
+    L = _lib.load()
+    rng = np.random.default_rng(33)
+    P = rng.random((1 << 16, 3)) - 0.5
+    t = kd.build_kdtree(P, leaf=16, boxsize=[1.0, 1.0, 1.0])
+    nq, k = (1 << 20) + 777, 5
+    Q = np.ascontiguousarray(rng.random((nq, 3)) - 0.5)
+    dd, di = kd.knn_search(t, torch.from_numpy(Q).cuda(), k)
+    dd, di = dd.cpu().numpy(), di.cpu().numpy()
+    vp = ctypes.c_void_p
+    hd = np.empty((nq, k))
+    hi = np.empty((nq, k), dtype=np.int64)
+    _lib.check(L.ckd_knn_host(t.handle, vp(Q.ctypes.data), nq, k, 1, vp(hd.ctypes.data),
+                              vp(hi.ctypes.data), None))
+    np.testing.assert_array_equal(hi, di)
+    np.testing.assert_array_equal(hd, dd)
+    pdist = torch.empty((nq, k), dtype=torch.float64, pin_memory=True)
+    pidx = torch.empty((nq, k), dtype=torch.int64, pin_memory=True)
+    _lib.check(L.ckd_knn_host(t.handle, vp(Q.ctypes.data), nq, k, 1, vp(pdist.data_ptr()),
+                              vp(pidx.data_ptr()), None))
+    np.testing.assert_array_equal(pidx.numpy(), di)
+    np.testing.assert_array_equal(pdist.numpy(), dd)
+    t.close()
