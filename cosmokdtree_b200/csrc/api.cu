@@ -127,6 +127,9 @@ ckd_status knn_run(const ckd_tree* t, const double* q, int64_t nq, int k, int so
 ckd_status knn_multi_k(const ckd_tree* t, const double* q, int64_t nq, const int32_t* kq,
                        int kmax, int sorted, double* dist, int64_t* idx, cudaStream_t s,
                        const ckd_mlp* net = nullptr, int64_t* nfb_out = nullptr);
+ckd_status knn_host_pipelined(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
+                              double* dist, int64_t* idx, cudaStream_t s);
+void release_host_staging();
 ckd_status knn_ordered(const ckd_tree* t, const double* q, const int32_t* order, int64_t nq, int k,
                        int sorted, double* dist, int64_t* idx, cudaStream_t s);
 ckd_status query_order(const ckd_tree* t, const double* q_dev, int64_t nq, int32_t* order,
@@ -384,6 +387,7 @@ ckd_status ckd_release_cached_memory(void) {
   CKD_CUDA(pool_for_current(&pool));
   CKD_CUDA(cudaDeviceSynchronize());
   CKD_CUDA(cudaMemPoolTrimTo(pool, 0));
+  release_host_staging();
   return CKD_OK;
 }
 
@@ -607,78 +611,8 @@ ckd_status ckd_knn_learned(const ckd_tree* t, const ckd_mlp* net, const double* 
   return knn_learned(t, net, q, nq, k, sorted, dist, idx, n_fallback, (cudaStream_t)stream);
 }
 
-// Host buffers from this many queries on: the search runs in row chunks on the
-// caller's stream while a second stream copies each finished chunk back (two device
-// result buffers in flight).  With pinned host buffers the whole pipeline is queued at
-// once; with pageable ones each copy returns when done, after the next chunk's search
-// has been queued, so the two still overlap.
+// Host buffers from this many queries on take the chunked pipeline (host_pipe.cu).
 constexpr int64_t kHostPipeRows = int64_t(1) << 20;
-constexpr int kHostPipeChunks = 16;
-
-static ckd_status knn_host_pipelined(const ckd_tree* t, const double* q, int64_t nq, int k,
-                                     int sorted, double* dist, int64_t* idx, cudaStream_t s) {
-  const int64_t rows = cdiv(nq, (int64_t)kHostPipeChunks);
-  const int d = t->d;
-  double *dq = nullptr, *dd[2] = {nullptr, nullptr};
-  int64_t* di[2] = {nullptr, nullptr};
-  cudaStream_t s2 = nullptr;
-  cudaEvent_t searched[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
-  struct Cleanup {
-    cudaStream_t s;
-    double** dq;
-    double** dd;
-    int64_t** di;
-    cudaStream_t* s2;
-    cudaEvent_t* ev;
-    ~Cleanup() {
-      if (*s2) cudaStreamSynchronize(*s2);
-      cudaStreamSynchronize(s);
-      dev_free(*dq, s);
-      for (int b = 0; b < 2; ++b) {
-        dev_free(dd[b], s);
-        dev_free(di[b], s);
-      }
-      for (int e = 0; e < 4; ++e)
-        if (ev[e]) cudaEventDestroy(ev[e]);
-      if (*s2) cudaStreamDestroy(*s2);
-    }
-  };
-  cudaEvent_t evs[4] = {nullptr, nullptr, nullptr, nullptr};
-  Cleanup cleanup{s, &dq, dd, di, &s2, evs};
-  CKD_CUDA(dev_alloc((void**)&dq, sizeof(double) * nq * d, s));
-  for (int b = 0; b < 2; ++b) {
-    CKD_CUDA(dev_alloc((void**)&dd[b], sizeof(double) * rows * k, s));
-    CKD_CUDA(dev_alloc((void**)&di[b], sizeof(int64_t) * rows * k, s));
-  }
-  CKD_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
-  for (int e = 0; e < 4; ++e) CKD_CUDA(cudaEventCreateWithFlags(&evs[e], cudaEventDisableTiming));
-  searched[0] = evs[0], searched[1] = evs[1], copied[0] = evs[2], copied[1] = evs[3];
-  CKD_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * nq * d, cudaMemcpyHostToDevice, s));
-  const int64_t nc = cdiv(nq, rows);
-  auto search = [&](int64_t c) -> ckd_status {
-    const int b = (int)(c & 1);
-    const int64_t r0 = c * rows, n = std::min(rows, nq - r0);
-    if (c >= 2) CKD_CUDA(cudaStreamWaitEvent(s, copied[b], 0));  // buffer b copied out
-    CKD_TRY(knn_run(t, dq + r0 * d, n, k, sorted, dd[b], di[b], s));
-    CKD_CUDA(cudaEventRecord(searched[b], s));
-    return CKD_OK;
-  };
-  CKD_TRY(search(0));
-  for (int64_t c = 0; c < nc; ++c) {
-    const int b = (int)(c & 1);
-    const int64_t r0 = c * rows, n = std::min(rows, nq - r0);
-    if (c + 1 < nc) CKD_TRY(search(c + 1));  // queued before this chunk's copy
-    CKD_CUDA(cudaStreamWaitEvent(s2, searched[b], 0));
-    CKD_CUDA(cudaMemcpyAsync(dist + r0 * k, dd[b], sizeof(double) * n * k,
-                             cudaMemcpyDeviceToHost, s2));
-    CKD_CUDA(cudaMemcpyAsync(idx + r0 * k, di[b], sizeof(int64_t) * n * k,
-                             cudaMemcpyDeviceToHost, s2));
-    CKD_CUDA(cudaEventRecord(copied[b], s2));
-  }
-  CKD_CUDA(cudaStreamSynchronize(s2));
-  CKD_CUDA(cudaStreamSynchronize(s));
-  return CKD_OK;
-}
 
 ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, int sorted,
                         double* dist, int64_t* idx, void* stream) {
@@ -688,7 +622,8 @@ ckd_status ckd_knn_host(const ckd_tree* t, const double* q, int64_t nq, int k, i
   if (nq == 0) return CKD_OK;
   if (!q || !dist || !idx) return fail(CKD_ERR_BAD_ARG, "null query or output pointer");
   cudaStream_t s = (cudaStream_t)stream;
-  if (nq >= kHostPipeRows) return knn_host_pipelined(t, q, nq, k, sorted, dist, idx, s);
+  if (nq >= kHostPipeRows && k <= (1 << 20))
+    return knn_host_pipelined(t, q, nq, k, sorted, dist, idx, s);
   double *dq = nullptr, *dd = nullptr;
   int64_t* di = nullptr;
   ckd_status st = CKD_OK;

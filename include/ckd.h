@@ -182,8 +182,10 @@ ckd_status ckd_knn_multi_k(const ckd_tree* tree, const double* q_dev, int64_t nq
 
 /* ckd_knn on host buffers (copies in, computes, copies out; synchronous).  From
  * 2^20 queries on, the search runs in 16 row chunks while a second stream copies
- * each finished chunk back (fastest with pinned output buffers; pageable ones
- * still overlap each copy with the next chunk's search). */
+ * each finished chunk back.  Pinned output buffers receive the copies directly;
+ * pageable ones are filled from a ring of pinned 32 MB slots that the library
+ * keeps between calls (released by ckd_release_cached_memory) by up to 16 host
+ * threads, while later pieces are in flight. */
 ckd_status ckd_knn_host(const ckd_tree* tree, const double* q_host, int64_t nq, int k, int sorted,
                         double* dist_host, int64_t* idx_host, void* stream);
 
