@@ -119,7 +119,21 @@ ckd_status knn_host_pipelined(const ckd_tree* t, const double* q, int64_t nq, in
                               double* dist, int64_t* idx, cudaStream_t s) {
   const int64_t rows = cdiv(nq, (int64_t)kChunks);
   const int d = t->d;
-  const bool direct = is_pinned(dist) && is_pinned(idx);
+  bool direct = is_pinned(dist) && is_pinned(idx);
+  // pageable outputs go through the pinned slot ring, held for the whole call; if
+  // no pinned memory can be had, the copies go straight to the pageable buffers
+  // (each then returns when done)
+  std::unique_lock<std::mutex> stage_lock(g_stage_mu, std::defer_lock);
+  if (!direct) {
+    stage_lock.lock();
+    if (!g_stage && cudaHostAlloc((void**)&g_stage, kSlotBytes * kSlots, cudaHostAllocDefault) !=
+                        cudaSuccess) {
+      cudaGetLastError();
+      g_stage = nullptr;
+      stage_lock.unlock();
+      direct = true;
+    }
+  }
   double *dq = nullptr, *dd[2] = {nullptr, nullptr};
   int64_t* di[2] = {nullptr, nullptr};
   cudaStream_t s2 = nullptr;
@@ -185,8 +199,6 @@ ckd_status knn_host_pipelined(const ckd_tree* t, const double* q, int64_t nq, in
     return CKD_OK;
   }
   // pageable outputs: pieces of `prow` rows through the pinned slot ring
-  std::lock_guard<std::mutex> lock(g_stage_mu);
-  if (!g_stage) CKD_CUDA(cudaHostAlloc((void**)&g_stage, kSlotBytes * kSlots, cudaHostAllocDefault));
   const int64_t prow = std::max<int64_t>(1, (int64_t)(kSlotBytes / (16 * (size_t)k)));
   struct Piece {
     int64_t c, r0, n;  // chunk, first row, rows
