@@ -119,8 +119,8 @@ ckd_status ckd_set_knn_variant(int variant);
  * searches (0 = automatic, default; 1 = always; 2 = never); key 7: inference of
  * the learned-bound network (0 = FP32 FMAs; 1 = tensor cores, tcgen05 MMAs on
  * BF16 activations, default); key 8: box search of up to 32768 boxes per call
- * (1 = a warp per box, frontier expanded a level at a time, default; 0 = a lane
- * per box); key 9: cap in MiB on the device memory the library's pool hands out
+ * on one tree, and of any number on a forest (1 = a warp per box, frontier
+ * expanded a level at a time, default; 0 = a lane per box); key 9: cap in MiB on the device memory the library's pool hands out
  * at any time on the current device (0 = none, default): an allocation past it
  * fails with CKD_ERR_OOM and the call returns everything it had taken; key 10:
  * how long (ms, default 20000) an idle CTA of the persistent forest launch waits
