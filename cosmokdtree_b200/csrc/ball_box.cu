@@ -550,7 +550,7 @@ constexpr int kBoxFront = 256;
 // points: 0.80 vs 4.8 ms).  Forest boxes always take the warp kernel: their trees are
 // clusters whose central boxes hold most of the points, and a lane per box leaves the
 // whole search waiting on the heaviest lanes (128k boxes on 2000 NFW trees: 25.4 vs
-// 40.8 ms, and 14.0 ms with the whole-subtree ranges above).
+// 40.8 ms, and 11.8 ms with the whole-subtree ranges above).
 constexpr int64_t kBoxWarpMax = 32768;
 
 template <int D, bool FILL>
@@ -576,12 +576,17 @@ __global__ void __launch_bounds__(128) k_box_warp(TreeView tv, const double* __r
   int64_t cur = FILL ? offsets[bi] : 0;
   const int64_t cur_end = FILL ? offsets[bi + 1] : 0;
   const int32_t root = broot ? broot[bi] : 0;
-  // points of one leaf, tested by the lanes and emitted in position order
-  auto scan_leaf = [&](int32_t st, int32_t ct) {
+  // points of one leaf, tested by the lanes and emitted in position order; a
+  // subtree inside the box (whole) is counted or emitted without the tests
+  auto scan_leaf = [&](int32_t st, int32_t ct, bool whole) {
+    if (!FILL && whole) {
+      cnt += ct;
+      return;
+    }
     for (int32_t b = 0; b < ct; b += 32) {
       const int32_t p = st + b + lane;
       bool in = b + lane < ct;
-      if (in) {
+      if (in && !whole) {
 #pragma unroll
         for (int j = 0; j < D; ++j) {
           const double x = __ldg(&tv.pts[(int64_t)j * tv.n + p]);
@@ -662,15 +667,17 @@ __global__ void __launch_bounds__(128) k_box_warp(TreeView tv, const double* __r
   }
   if (!overflow) {
     for (int c0 = 0; c0 < nf; c0 += 32) {
-      int32_t st_l = 0, ct_l = 0;
+      int32_t st_l = 0, ct_l = 0, wh_l = 0;
       if (c0 + lane < nf) {
         const NodeMeta m = load_meta(tv.meta, ~front[w][fb][c0 + lane]);
         st_l = m.start;
         ct_l = m.count;
+        wh_l = m.left >= 0;  // an internal node in the frontier lies inside the box
       }
       const int nl = min(32, nf - c0);
       for (int i = 0; i < nl; ++i)
-        scan_leaf(__shfl_sync(FULL, st_l, i), __shfl_sync(FULL, ct_l, i));
+        scan_leaf(__shfl_sync(FULL, st_l, i), __shfl_sync(FULL, ct_l, i),
+                  __shfl_sync(FULL, wh_l, i) != 0);
     }
   } else {  // depth-first walk, left child first (stack depth <= tree depth + 2)
     int top = 0;
@@ -682,7 +689,7 @@ __global__ void __launch_bounds__(128) k_box_warp(TreeView tv, const double* __r
       __syncwarp();
       const NodeMeta m = load_meta(tv.meta, node);
       if (m.left < 0) {
-        scan_leaf(m.start, m.count);
+        scan_leaf(m.start, m.count, false);
       } else {
         double bl = 0.0, bh = 0.0;
 #pragma unroll
@@ -693,7 +700,7 @@ __global__ void __launch_bounds__(128) k_box_warp(TreeView tv, const double* __r
           }
         const bool gr = bh > m.split, gl = bl < m.split;
         if (gl && gr && m.count >= kBoxWholeMin && box_holds_node<D>(tv, node, lo, hi)) {
-          scan_leaf(m.start, m.count);
+          scan_leaf(m.start, m.count, true);
           continue;
         }
         if (lane == 0) {
